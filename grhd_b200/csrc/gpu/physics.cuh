@@ -1,0 +1,723 @@
+// physics.cuh -- pointwise GRHD physics for the sm_100a kernels.
+//
+// Every routine restates one reference routine (file:line in RuelasF/GRHD) with the
+// reference's evaluation order; built with --fmad=false the FP64 instantiation rounds
+// exactly as the reference's operation sequence does.  The arithmetic type R is double
+// for the parity path and float for the reconstruction/Riemann/source part of the mixed
+// policy; con2prim is always double.
+//
+// Processor-dependent Fortran semantics, fixed the same way in the CPU oracle:
+//   MAX/MIN with NaN arguments keep the first non-NaN value (m=a; if (b>m || m!=m) m=b).
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+namespace grhd {
+
+constexpr int NEQ = 5;
+constexpr int EQ_DE = 0, EQ_PR = 1, EQ_VX = 2, EQ_VY = 3, EQ_VZ = 4;
+constexpr int REC_GODUNOV = 1, REC_TVD = 2, REC_WENO3 = 3, REC_MP5 = 4, REC_WENO5 = 5;
+constexpr int RS_HLLE = 1, RS_HLLC = 2;
+constexpr int LIM_MINMOD = 1, LIM_SUPERBEE = 2, LIM_MC = 3;
+
+// recon branch codes (one per face: the reference's conditions do not depend on the variable)
+constexpr int BR_GODUNOV = 0, BR_TVD = 1, BR_TVD_MC = 2, BR_WENO3 = 3, BR_MP5 = 4, BR_WENO5 = 5;
+
+struct Phys {
+  int rec, lim, rs, sensor;
+  int nonmink;  // metric_type /= 'Minkowski' (reconstruction.f90:356 etc.)
+  int srhd;     // Minkowski + Cartesian: SRHD wavespeeds and no sources (fluxes.f90:45, equations.f90:521)
+  double adb, g1, rho_floor, p_floor, v_max;
+};
+
+// per-face metric (k-invariant): lapse, normal shift, symmetric gamma_ij, sqrt(gamma), gamma^dd
+template <class R>
+struct FaceMetric {
+  R alpha, beta_n, g11, g12, g13, g22, g23, g33, sqg, gup;
+  __device__ __forceinline__ R G(int a, int b) const {  // 1-based symmetric access
+    const int m = a < b ? a * 4 + b : b * 4 + a;
+    switch (m) {
+      case 5: return g11; case 6: return g12; case 7: return g13;
+      case 10: return g22; case 11: return g23; default: return g33;
+    }
+  }
+};
+
+template <class R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a || a != a) ? b : a; }
+template <class R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a || a != a) ? b : a; }
+template <class R> __device__ __forceinline__ R sgn1(R x) { return copysign(R(1), x); }
+template <class R> __device__ __forceinline__ bool fin(R x) { return isfinite(x); }
+template <class R> __device__ __forceinline__ R tiny_of();
+template <> __device__ __forceinline__ double tiny_of<double>() { return DBL_MIN; }
+template <> __device__ __forceinline__ float tiny_of<float>() { return FLT_MIN; }
+template <class R> __device__ __forceinline__ R eps_of();
+template <> __device__ __forceinline__ double eps_of<double>() { return DBL_EPSILON; }
+template <> __device__ __forceinline__ float eps_of<float>() { return FLT_EPSILON; }
+
+// ------------------------------------------------------------------------------------
+// reconstruction.f90:28-278
+// ------------------------------------------------------------------------------------
+template <class R> __device__ __forceinline__ R minmod_2(R a, R b) {
+  return R(0.5) * (sgn1(a) + sgn1(b)) * rmin(fabs(a), fabs(b));
+}
+template <class R> __device__ __forceinline__ R minmod_3(R a, R b, R c) {
+  return sgn1(a) * rmax(R(0), rmin(rmin(fabs(a), sgn1(a) * b), sgn1(a) * c));
+}
+template <class R> __device__ __forceinline__ R minmod_4(R a, R b, R c, R d) {
+  return R(0.125) * (sgn1(a) + sgn1(b)) * fabs(sgn1(a) + sgn1(c)) * fabs(sgn1(a) + sgn1(d)) *
+         rmin(rmin(rmin(fabs(a), fabs(b)), fabs(c)), fabs(d));
+}
+// reconstruction.f90:141-181, q(-1:1)
+template <class R> __device__ __forceinline__ R weno3(R qm, R q0, R qp) {
+  const R eps_min = R(1.0e-14);
+  const R d0 = R(2.0 / 3.0), d1 = R(1.0 / 3.0);
+  R p0 = R(0.5) * q0 + R(0.5) * qp;
+  R p1 = R(-0.5) * qm + R(1.5) * q0;
+  R t0 = q0 - qp, t1 = qm - q0;
+  R b0 = t0 * t0, b1 = t1 * t1;
+  R sensor = fabs(b0 - b1) / (rmax(b0, b1) + eps_min);
+  R eh = eps_min + (qm * qm + q0 * q0 + qp * qp) * exp(R(-10) * sensor);
+  R e0 = eh + b0, e1 = eh + b1;
+  R a0 = d0 / (e0 * e0), a1 = d1 / (e1 * e1);
+  R w0 = a0 / (a0 + a1), w1 = a1 / (a0 + a1);
+  return w0 * p0 + w1 * p1;
+}
+// reconstruction.f90:187-215, q(-2:2)
+template <class R> __device__ __forceinline__ R weno5(R q_2, R q_1, R q0, R q1, R q2) {
+  const R eps = R(1.0e-14);
+  const R d0 = R(0.3), d1 = R(0.6), d2 = R(0.1);
+  const R c1312 = R(13.0 / 12.0);
+  R a, b;
+  a = q0 - R(2) * q1 + q2; b = R(3) * q0 - R(4) * q1 + q2;
+  R b0 = c1312 * (a * a) + R(0.25) * (b * b);
+  a = q_1 - R(2) * q0 + q1; b = q_1 - q1;
+  R b1 = c1312 * (a * a) + R(0.25) * (b * b);
+  a = q_2 - R(2) * q_1 + q0; b = q_2 - R(4) * q_1 + R(3) * q0;
+  R b2 = c1312 * (a * a) + R(0.25) * (b * b);
+  R tau5 = fabs(b0 - b2);
+  R a0 = d0 * (R(1) + (tau5 / (eps + b0)));
+  R a1 = d1 * (R(1) + (tau5 / (eps + b1)));
+  R a2 = d2 * (R(1) + (tau5 / (eps + b2)));
+  R s = a0 + a1 + a2;
+  R w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+  R p0 = R(1.0 / 3.0) * q0 + R(5.0 / 6.0) * q1 - R(1.0 / 6.0) * q2;
+  R p1 = -(R(1.0 / 6.0) * q_1) + R(5.0 / 6.0) * q0 + R(1.0 / 3.0) * q1;
+  R p2 = R(1.0 / 3.0) * q_2 - R(7.0 / 6.0) * q_1 + R(11.0 / 6.0) * q0;
+  return w0 * p0 + w1 * p1 + w2 * p2;
+}
+// reconstruction.f90:222-254, q(-2:2)
+template <class R> __device__ __forceinline__ R mp5(R q_2, R q_1, R q0, R q1, R q2) {
+  const R alpha = R(4), eps = R(1.0e-10);
+  R val_L = (R(2) * q_2 - R(13) * q_1 + R(47) * q0 + R(27) * q1 - R(3) * q2) / R(60);
+  R val_mp = q0 + minmod_2(q1 - q0, alpha * (q0 - q_1));
+  if ((val_L - q0) * (val_L - val_mp) < eps) return val_L;
+  R d_jm1 = q_2 - R(2) * q_1 + q0;
+  R d_j = q_1 - R(2) * q0 + q1;
+  R d_jp1 = q0 - R(2) * q1 + q2;
+  R dm4_jph = minmod_4(R(4) * d_j - d_jp1, R(4) * d_jp1 - d_j, d_j, d_jp1);
+  R dm4_jmh = minmod_4(R(4) * d_j - d_jm1, R(4) * d_jm1 - d_j, d_j, d_jm1);
+  R val_ul = q0 + alpha * (q0 - q_1);
+  R val_av = R(0.5) * (q0 + q1);
+  R val_md = val_av - R(0.5) * dm4_jph;
+  R val_lc = q0 + R(0.5) * (q0 - q_1) + R(4) * dm4_jmh / R(3);
+  R vmin = rmax(rmin(rmin(q0, q1), val_md), rmin(rmin(q0, val_ul), val_lc));
+  R vmax = rmin(rmax(rmax(q0, q1), val_md), rmax(rmax(q0, val_ul), val_lc));
+  return val_L + minmod_2(vmin - val_L, vmax - val_L);
+}
+// reconstruction.f90:259-278
+template <class R> __device__ __forceinline__ R tvd_slope(R a, R b, int lim) {
+  if (lim == LIM_SUPERBEE) {
+    if (a * b <= R(0)) return R(0);
+    return sgn1(a) * rmax(rmin(R(2) * fabs(a), fabs(b)), rmin(fabs(a), R(2) * fabs(b)));
+  }
+  if (lim == LIM_MC) return minmod_3(R(2) * b, R(0.5) * (a + b), R(2) * a);
+  return minmod_2(a, b);
+}
+
+// Cells [lo, hi] of the 6-point window (i-2 .. i+3 for face i) that a scheme reads.
+__host__ __device__ __forceinline__ void stencil_range(int rec, int sensor, int &lo, int &hi) {
+  if (rec == REC_GODUNOV) { lo = 2; hi = 3; }
+  else if (rec == REC_TVD || rec == REC_WENO3) { lo = sensor ? 0 : 1; hi = 4; }
+  else { lo = 0; hi = 5; }
+}
+
+// reconstruct_1d_core branch selection for face i (reconstruction.f90:318-645).
+// w[v][m] = prim(v, i-2+m).
+template <class R>
+__device__ __forceinline__ int recon_branch(const Phys &P, const R (&w)[NEQ][6], int i, int nodes, int dir) {
+  R p_jump = R(0), rho_jump = R(0);
+  if (P.rec != REC_GODUNOV && P.sensor) {
+    R pmax = w[EQ_PR][0], pmin = w[EQ_PR][0], rmx = w[EQ_DE][0], rmn = w[EQ_DE][0];
+#pragma unroll
+    for (int m = 1; m < 5; ++m) {
+      pmax = rmax(pmax, w[EQ_PR][m]); pmin = rmin(pmin, w[EQ_PR][m]);
+      rmx = rmax(rmx, w[EQ_DE][m]); rmn = rmin(rmn, w[EQ_DE][m]);
+    }
+    const R pf = R(P.p_floor), rf = R(P.rho_floor);
+    p_jump = (pmax > R(1.0e3) * pf) ? (pmax - pmin) / rmax(pmin, pf) : R(0);
+    rho_jump = (rmx > R(1.0e3) * rf) ? (rmx - rmn) / rmax(rmn, rf) : R(0);
+  }
+  const bool inner = P.nonmink && dir == 1 && i <= 0;
+  const R atm = R(1.0e2) * R(P.rho_floor);
+  const bool atmo = w[EQ_DE][2] <= atm || w[EQ_DE][3] <= atm;
+  const bool cliff = p_jump >= R(10.0) || rho_jump >= R(10.0);
+  const bool shock = p_jump >= R(0.80) || rho_jump >= R(0.50);
+  const bool smooth_break = p_jump >= R(0.40) || rho_jump >= R(0.15);
+  switch (P.rec) {
+    case REC_GODUNOV: return BR_GODUNOV;
+    case REC_TVD:
+      if (P.sensor && (inner || atmo || cliff)) return BR_GODUNOV;
+      return BR_TVD;
+    case REC_WENO3:
+      if (P.sensor) {
+        if (inner || atmo || cliff) return BR_GODUNOV;
+        if (shock) return BR_TVD_MC;
+        return BR_WENO3;
+      }
+      return inner ? BR_GODUNOV : BR_WENO3;
+    case REC_MP5:
+      if (P.sensor) {
+        if (inner || atmo || cliff) return BR_GODUNOV;
+        if (shock) return BR_TVD_MC;
+        if (smooth_break || (P.nonmink && dir == 1 && i <= 3) ||
+            (P.nonmink && dir == 2 && (i <= 2 || i >= nodes - 2)))
+          return BR_WENO3;
+        return BR_MP5;
+      }
+      return inner ? BR_GODUNOV : BR_MP5;
+    default:
+      if (P.sensor) {
+        if (inner || atmo || cliff) return BR_GODUNOV;
+        if (shock) return BR_TVD_MC;
+        if (smooth_break) return BR_WENO3;
+        return BR_WENO5;
+      }
+      return inner ? BR_GODUNOV : BR_WENO5;
+  }
+}
+
+// interface states of one variable for a branch
+template <class R>
+__device__ __forceinline__ void recon_var(int br, int lim, const R (&s)[6], R &qL, R &qR) {
+  switch (br) {
+    case BR_GODUNOV: qL = s[2]; qR = s[3]; break;
+    case BR_TVD:
+    case BR_TVD_MC: {
+      const int l = (br == BR_TVD) ? lim : LIM_MC;
+      qL = s[2] + R(0.5) * tvd_slope(s[2] - s[1], s[3] - s[2], l);
+      qR = s[3] - R(0.5) * tvd_slope(s[3] - s[2], s[4] - s[3], l);
+      break;
+    }
+    case BR_WENO3: qL = weno3(s[1], s[2], s[3]); qR = weno3(s[4], s[3], s[2]); break;
+    case BR_MP5: qL = mp5(s[0], s[1], s[2], s[3], s[4]); qR = mp5(s[5], s[4], s[3], s[2], s[1]); break;
+    default: qL = weno5(s[0], s[1], s[2], s[3], s[4]); qR = weno5(s[5], s[4], s[3], s[2], s[1]); break;
+  }
+}
+
+// reconstruction.f90:647-655 positivity floors; returns the number of values raised
+template <class R>
+__device__ __forceinline__ int recon_floors(const Phys &P, R (&qL)[NEQ], R (&qR)[NEQ]) {
+  const R rf = R(P.rho_floor), pf = R(P.p_floor);
+  int n = 0;
+  n += !(qL[EQ_DE] >= rf); qL[EQ_DE] = rmax(qL[EQ_DE], rf);
+  n += !(qR[EQ_DE] >= rf); qR[EQ_DE] = rmax(qR[EQ_DE], rf);
+  n += !(qL[EQ_PR] >= pf); qL[EQ_PR] = rmax(qL[EQ_PR], pf);
+  n += !(qR[EQ_PR] >= pf); qR[EQ_PR] = rmax(qR[EQ_PR], pf);
+  return n;
+}
+
+// ------------------------------------------------------------------------------------
+// equations.f90:434-502, fluxes.f90:76-156, 669-803
+// ------------------------------------------------------------------------------------
+// velocity cap shared by calc_fluxes, prim_to_cons_face and the wavespeed routines
+template <class R>
+__device__ __forceinline__ R cap_velocity(const FaceMetric<R> &m, R (&v)[3], R v_max) {
+  R vsq = R(0);
+#pragma unroll
+  for (int a = 1; a <= 3; ++a)
+#pragma unroll
+    for (int b = 1; b <= 3; ++b) vsq = vsq + m.G(a, b) * v[a - 1] * v[b - 1];
+  if (vsq >= v_max) {
+    v[0] = v[0] * sqrt(v_max / vsq);
+    v[1] = v[1] * sqrt(v_max / vsq);
+    v[2] = v[2] * sqrt(v_max / vsq);
+    vsq = v_max;
+  }
+  return vsq;
+}
+template <class R>
+__device__ __forceinline__ void lower(const FaceMetric<R> &m, const R (&v)[3], R (&vc)[3]) {
+#pragma unroll
+  for (int a = 1; a <= 3; ++a) {
+    R s = R(0);
+#pragma unroll
+    for (int b = 1; b <= 3; ++b) s = s + m.G(a, b) * v[b - 1];
+    vc[a - 1] = s;
+  }
+}
+
+// calc_fluxes (F) and prim_to_cons_face (U) together: they share v_sq, h, W, v_cov
+template <class R>
+__device__ __forceinline__ void flux_and_cons(const Phys &P, const R (&q)[NEQ], int dir,
+                                              const FaceMetric<R> &m, R (&f)[NEQ], R (&u)[NEQ]) {
+  R v[3] = {q[EQ_VX], q[EQ_VY], q[EQ_VZ]}, vc[3];
+  const R vsq = cap_velocity(m, v, R(P.v_max));
+  lower(m, v, vc);
+  const R v_norm = dir == 1 ? v[0] : (dir == 2 ? v[1] : v[2]);
+  const R h = R(1) + R(P.g1) * q[EQ_PR] / q[EQ_DE];
+  const R W = R(1) / sqrt(R(1) - vsq);
+  const R v_eff = m.alpha * v_norm - m.beta_n;
+  const R rhW2 = q[EQ_DE] * h * (W * W);
+  f[EQ_DE] = q[EQ_DE] * W * v_eff;
+  f[EQ_PR] = rhW2 * v_eff + q[EQ_PR] * m.beta_n - f[EQ_DE];
+  f[EQ_VX] = rhW2 * vc[0] * v_eff + (dir == 1 ? m.alpha * q[EQ_PR] : R(0));
+  f[EQ_VY] = rhW2 * vc[1] * v_eff + (dir == 2 ? m.alpha * q[EQ_PR] : R(0));
+  f[EQ_VZ] = rhW2 * vc[2] * v_eff + (dir == 3 ? m.alpha * q[EQ_PR] : R(0));
+  u[EQ_DE] = q[EQ_DE] * W;
+  u[EQ_PR] = rhW2 - q[EQ_PR] - q[EQ_DE] * W;
+  u[EQ_VX] = rhW2 * vc[0];
+  u[EQ_VY] = rhW2 * vc[1];
+  u[EQ_VZ] = rhW2 * vc[2];
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) { f[n] = f[n] * m.sqg; u[n] = u[n] * m.sqg; }
+}
+
+// calc_wavespeeds_srhd / calc_wavespeeds_grhd; gamma^dd of the face comes precomputed
+// with the reference's Cramer formula (fluxes.f90:760-774)
+template <class R>
+__device__ __forceinline__ void wavespeeds(const Phys &P, const R (&q)[NEQ], int dir,
+                                           const FaceMetric<R> &m, R &wmin, R &wmax) {
+  R v[3] = {q[EQ_VX], q[EQ_VY], q[EQ_VZ]};
+  const R vsq = cap_velocity(m, v, R(P.v_max));
+  const R enth = R(1) + R(P.g1) * q[EQ_PR] / q[EQ_DE];
+  const R cs2 = R(P.adb) * q[EQ_PR] / (q[EQ_DE] * enth);
+  const R cs = sqrt(cs2);
+  const R vn = dir == 1 ? v[0] : (dir == 2 ? v[1] : v[2]);
+  R e1, e2, e3;
+  if (P.srhd) {
+    const R t1 = R(1) / (R(1) - vsq * cs2);
+    const R t2 = cs * sqrt((R(1) - vsq) * (R(1) / t1 - (vn * vn) * (R(1) - cs2)));
+    e1 = vn;
+    e2 = t1 * (vn * (R(1) - cs2) + t2);
+    e3 = t1 * (vn * (R(1) - cs2) - t2);
+  } else {
+    const R t1 = m.alpha / (R(1) - vsq * cs2);
+    const R t2 = cs * sqrt(rmax(R(0), (R(1) - vsq) * (m.gup * (R(1) - vsq * cs2) - (vn * vn) * (R(1) - cs2))));
+    e1 = m.alpha * vn - m.beta_n;
+    e2 = t1 * (vn * (R(1) - cs2) + t2) - m.beta_n;
+    e3 = t1 * (vn * (R(1) - cs2) - t2) - m.beta_n;
+  }
+  wmax = rmax(rmax(rmax(R(0), e1), e2), e3);
+  wmin = rmin(rmin(rmin(R(0), e1), e2), e3);
+}
+
+// calc_hlle_fluxes, fluxes.f90:125-156
+template <class R>
+__device__ __forceinline__ void hlle(const Phys &P, const R (&qL)[NEQ], const R (&qR)[NEQ], int dir,
+                                     const FaceMetric<R> &m, R (&flux)[NEQ]) {
+  R fL[NEQ], fR[NEQ], uL[NEQ], uR[NEQ], lLmin, lLmax, lRmin, lRmax;
+  flux_and_cons(P, qL, dir, m, fL, uL);
+  flux_and_cons(P, qR, dir, m, fR, uR);
+  wavespeeds(P, qL, dir, m, lLmin, lLmax);
+  wavespeeds(P, qR, dir, m, lRmin, lRmax);
+  const R ap = rmax(rmax(R(0), lLmax), lRmax);
+  const R am = rmin(rmin(R(0), lLmin), lRmin);
+  if (fabs(ap - am) < R(1.0e-14)) {
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) flux[n] = R(0);
+  } else {
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) flux[n] = (ap * fL[n] - am * fR[n] + ap * am * (uR[n] - uL[n])) / (ap - am);
+  }
+}
+
+// Orthonormal face frame of build_face_orthonormal_frame (fluxes.f90:402-473), precomputed
+// per face: cof[a][i] = coframe(a+1,i+1), gup = gamma^dd, ok flag.
+template <class R>
+struct FaceFrame {
+  R cof[3][3];
+  R gup;
+  int ok;
+};
+
+// fluxes.f90:509-568 calc_srhd_local_state
+template <class R>
+__device__ __forceinline__ bool srhd_local(const Phys &P, const R (&ql)[NEQ], R (&u)[NEQ], R (&f)[NEQ],
+                                           R &wmin, R &wmax) {
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) { u[n] = R(0); f[n] = R(0); }
+  wmin = R(0); wmax = R(0);
+  const R rho = ql[EQ_DE], pr = ql[EQ_PR], v0 = ql[EQ_VX], v1 = ql[EQ_VY], v2 = ql[EQ_VZ];
+  if (!fin(rho) || !fin(pr) || !fin(v0) || !fin(v1) || !fin(v2) || rho <= R(0) || pr < R(0)) return false;
+  const R vsq = v0 * v0 + v1 * v1 + v2 * v2;
+  if (!fin(vsq) || vsq < R(0)) return false;
+  if (vsq >= R(P.v_max)) return false;
+  const R h = R(1) + R(P.g1) * pr / rho;
+  if (!fin(h) || h <= R(0)) return false;
+  const R cs2 = R(P.adb) * pr / (rho * h);
+  if (!fin(cs2) || cs2 < R(0) || cs2 >= R(1)) return false;
+  const R W = R(1) / sqrt(R(1) - vsq);
+  const R D = rho * W;
+  const R rhW2 = rho * h * (W * W);
+  const R m0 = rhW2 * v0, m1 = rhW2 * v1, m2 = rhW2 * v2;
+  u[EQ_DE] = D; u[EQ_PR] = rhW2 - pr - D; u[EQ_VX] = m0; u[EQ_VY] = m1; u[EQ_VZ] = m2;
+  f[EQ_DE] = D * v0;
+  f[EQ_PR] = m0 - D * v0;
+  f[EQ_VX] = m0 * v0 + pr;
+  f[EQ_VY] = m1 * v0;
+  f[EQ_VZ] = m2 * v0;
+  const R den = R(1) - vsq * cs2;
+  const R rad = (R(1) - vsq) * (R(1) - vsq * cs2 - (v0 * v0) * (R(1) - cs2));
+  if (den <= R(1.0e-14) || rad < R(-1.0e-12)) return false;
+  const R ac = sqrt(cs2) * sqrt(rmax(R(0), rad));
+  wmin = (v0 * (R(1) - cs2) - ac) / den;
+  wmax = (v0 * (R(1) - cs2) + ac) / den;
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) if (!fin(u[n]) || !fin(f[n])) return false;
+  if (!fin(wmin) || !fin(wmax)) return false;
+  return true;
+}
+
+// fluxes.f90:571-591
+template <class R>
+__device__ __forceinline__ bool admissible(const R (&u)[NEQ]) {
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) if (!fin(u[n])) return false;
+  if (u[EQ_DE] <= R(0)) return false;
+  const R E = u[EQ_PR] + u[EQ_DE];
+  const R msq = u[EQ_VX] * u[EQ_VX] + u[EQ_VY] * u[EQ_VY] + u[EQ_VZ] * u[EQ_VZ];
+  const R scale = rmax(rmax(tiny_of<R>(), E * E), u[EQ_DE] * u[EQ_DE] + msq);
+  if (E <= R(0)) return false;
+  if (E * E - u[EQ_DE] * u[EQ_DE] - msq <= R(1.0e-13) * scale) return false;
+  return true;
+}
+
+// fluxes.f90:596-624
+template <class R>
+__device__ __forceinline__ bool local_to_coord(const R (&ul)[NEQ], const R (&fl)[NEQ], R w, R alpha,
+                                               R sqg, const FaceFrame<R> &fr, R (&flux)[NEQ]) {
+  R mf[NEQ];
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) { flux[n] = R(0); mf[n] = fl[n] - w * ul[n]; }
+  const R factor = sqg * alpha * sqrt(fr.gup);
+  if (!fin(factor)) return false;
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) if (!fin(mf[n])) return false;
+  flux[EQ_DE] = factor * mf[EQ_DE];
+  flux[EQ_PR] = factor * mf[EQ_PR];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    R s = R(0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) s = s + factor * fr.cof[a][i] * mf[EQ_VX + a];
+    flux[EQ_VX + i] = s;
+  }
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) if (!fin(flux[n])) return false;
+  return true;
+}
+
+// calc_hllc_fluxes, fluxes.f90:174-397.  Returns true when it fell back to HLLE.
+template <class R>
+__device__ bool hllc(const Phys &P, const R (&qL)[NEQ], const R (&qR)[NEQ], int dir,
+                     const FaceMetric<R> &m, const FaceFrame<R> &fr, R (&flux)[NEQ]) {
+  const R alpha = m.alpha, sqg = m.sqg;
+  R qLh[NEQ], qRh[NEQ], uL[NEQ], uR[NEQ], fL[NEQ], fR[NEQ];
+  R lLmin, lLmax, lRmin, lRmax;
+  R ls, denom, face_speed, lam_l, lam_r;
+  if (!(alpha > R(0)) || !(sqg > R(0)) || !fin(alpha) || !fin(sqg) || !fr.ok) goto fallback;
+  // primitives_to_local_frame (fluxes.f90:490-504)
+#pragma unroll
+  for (int n = 0; n < 2; ++n) { qLh[n] = qL[n]; qRh[n] = qR[n]; }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    R sl = R(0), sr = R(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { sl = sl + fr.cof[a][i] * qL[EQ_VX + i]; sr = sr + fr.cof[a][i] * qR[EQ_VX + i]; }
+    qLh[EQ_VX + a] = sl; qRh[EQ_VX + a] = sr;
+  }
+  if (!srhd_local(P, qLh, uL, fL, lLmin, lLmax)) goto fallback;
+  if (!srhd_local(P, qRh, uR, fR, lRmin, lRmax)) goto fallback;
+  lam_l = rmin(lLmin, lRmin);
+  lam_r = rmax(lLmax, lRmax);
+  face_speed = m.beta_n / (alpha * sqrt(fr.gup));
+  if (!fin(face_speed) || lam_r - lam_l <= R(1.0e-13)) goto fallback;
+  if (face_speed <= lam_l) {
+    if (!local_to_coord(uL, fL, face_speed, alpha, sqg, fr, flux)) goto fallback;
+    return false;
+  } else if (face_speed >= lam_r) {
+    if (!local_to_coord(uR, fR, face_speed, alpha, sqg, fr, flux)) goto fallback;
+    return false;
+  }
+  {
+    R uh[NEQ], fh[NEQ];
+    denom = lam_r - lam_l;
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) {
+      uh[n] = (lam_r * uR[n] - lam_l * uL[n] + fL[n] - fR[n]) / denom;
+      fh[n] = (lam_r * fL[n] - lam_l * fR[n] + lam_r * lam_l * (uR[n] - uL[n])) / denom;
+    }
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) if (!fin(uh[n]) || !fin(fh[n])) goto fallback;
+    const R E_hll = uh[EQ_PR] + uh[EQ_DE];
+    const R FE_hll = fh[EQ_PR] + fh[EQ_DE];
+    const R A = FE_hll, B = -(E_hll + fh[EQ_VX]), Cq = uh[EQ_VX];
+    R disc = B * B - R(4) * A * Cq;
+    const R disc_scale = rmax(rmax(tiny_of<R>(), B * B), fabs(R(4) * A * Cq));
+    if (!fin(disc) || disc < R(-1.0e-12) * disc_scale) goto fallback;
+    disc = rmax(R(0), disc);
+    const R coef_scale = rmax(rmax(tiny_of<R>(), fabs(B)), fabs(Cq));
+    const bool quad = fabs(A) > R(1.0e-13) * coef_scale;
+    if (!quad) {
+      if (fabs(B) <= R(1.0e-14) * rmax(tiny_of<R>(), fabs(Cq))) goto fallback;
+      ls = -Cq / B;
+    } else {
+      denom = -B - sqrt(disc);
+      if (fabs(denom) > R(1.0e-14) * rmax(rmax(tiny_of<R>(), fabs(B)), sqrt(disc))) {
+        ls = denom / (R(2) * A);
+      } else {
+        denom = -B + sqrt(disc);
+        if (fabs(denom) <= R(1.0e-14) * rmax(rmax(tiny_of<R>(), fabs(B)), sqrt(disc))) goto fallback;
+        ls = (R(2) * Cq) / denom;
+      }
+    }
+    const R root_tol = R(1.0e-10) * rmax(rmax(R(1), fabs(lam_l)), fabs(lam_r));
+    bool valid = fin(ls) && ls >= lam_l - root_tol && ls <= lam_r + root_tol && fabs(ls) <= R(1) + root_tol;
+    if (!valid && quad) {
+      const R alt = (-B + sqrt(disc)) / (R(2) * A);
+      if (fin(alt) && alt >= lam_l - root_tol && alt <= lam_r + root_tol && fabs(alt) <= R(1) + root_tol) {
+        ls = alt;
+        valid = true;
+      }
+    }
+    if (!valid) goto fallback;
+    ls = rmin(lam_r, rmax(lam_l, ls));
+    const R A_l = lam_l * (uL[EQ_PR] + uL[EQ_DE]) - uL[EQ_VX];
+    const R B_l = uL[EQ_VX] * (lam_l - qLh[EQ_VX]) - qLh[EQ_PR];
+    const R A_r = lam_r * (uR[EQ_PR] + uR[EQ_DE]) - uR[EQ_VX];
+    const R B_r = uR[EQ_VX] * (lam_r - qRh[EQ_VX]) - qRh[EQ_PR];
+    denom = R(1) - lam_l * ls;
+    if (fabs(denom) <= R(1.0e-13)) goto fallback;
+    const R psl = (A_l * ls - B_l) / denom;
+    denom = R(1) - lam_r * ls;
+    if (fabs(denom) <= R(1.0e-13)) goto fallback;
+    const R psr = (A_r * ls - B_r) / denom;
+    const R state_scale = rmax(rmax(rmax(rmax(tiny_of<R>(), fabs(uL[EQ_PR] + uL[EQ_DE])), fabs(uR[EQ_PR] + uR[EQ_DE])),
+                                    fabs(uL[EQ_VX])), fabs(uR[EQ_VX]));
+    const R ptol = R(1.0e-8) * rmax(rmax(rmax(rmax(tiny_of<R>(), fabs(qLh[EQ_PR])), fabs(qRh[EQ_PR])), fabs(psl)), fabs(psr)) +
+                   R(1.0e2) * eps_of<R>() * state_scale;
+    if (!fin(psl) || !fin(psr) || fabs(psl - psr) > ptol) goto fallback;
+    const R ps = R(0.5) * (psl + psr);
+    if (!fin(ps) || fabs(lam_l - ls) <= R(1.0e-13) || fabs(lam_r - ls) <= R(1.0e-13)) goto fallback;
+    R usL[NEQ], usR[NEQ], fsL[NEQ], fsR[NEQ];
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) {
+      const R pv = (n == EQ_PR) ? ls : ((n == EQ_VX) ? R(1) : R(0));
+      usL[n] = (lam_l * uL[n] - fL[n] + ps * pv) / (lam_l - ls);
+      usR[n] = (lam_r * uR[n] - fR[n] + ps * pv) / (lam_r - ls);
+    }
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) {
+      fsL[n] = fL[n] + lam_l * (usL[n] - uL[n]);
+      fsR[n] = fR[n] + lam_r * (usR[n] - uR[n]);
+    }
+    if (!admissible(usL) || !admissible(usR)) goto fallback;
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) if (!fin(fsL[n]) || !fin(fsR[n])) goto fallback;
+    bool ok;
+    if (face_speed <= ls) ok = local_to_coord(usL, fsL, face_speed, alpha, sqg, fr, flux);
+    else ok = local_to_coord(usR, fsR, face_speed, alpha, sqg, fr, flux);
+    if (!ok) goto fallback;
+    return false;
+  }
+fallback:
+  hlle(P, qL, qR, dir, m, flux);
+  return true;
+}
+
+// ------------------------------------------------------------------------------------
+// equations.f90:94-424 con2prim (always FP64)
+// ------------------------------------------------------------------------------------
+struct CellMetric {  // symmetric gamma_ij and gamma^ij, sqrt(gamma)
+  double g11, g12, g13, g22, g23, g33;
+  double i11, i12, i13, i22, i23, i33;
+  double sqg;
+};
+
+enum C2PFlags : unsigned {
+  C2P_FLOOR_PRE = 1u, C2P_CAUSAL = 2u, C2P_BRENT = 4u, C2P_ROOT_FAIL = 8u, C2P_BAD_V = 16u, C2P_SANITISE = 32u
+};
+
+__device__ __forceinline__ double qsq(const CellMetric &m, double S1, double S2, double S3) {
+  // sum over (ii, jj) in the reference's loop order (equations.f90:273-277, :236-242)
+  double s = 0.0;
+  s = s + m.i11 * S1 * S1; s = s + m.i12 * S1 * S2; s = s + m.i13 * S1 * S3;
+  s = s + m.i12 * S2 * S1; s = s + m.i22 * S2 * S2; s = s + m.i23 * S2 * S3;
+  s = s + m.i13 * S3 * S1; s = s + m.i23 * S3 * S2; s = s + m.i33 * S3 * S3;
+  return s;
+}
+// equations.f90:212-246
+__device__ __forceinline__ void residual(double g1, double W, double D, double tau, double Q2,
+                                         double &res, double &dres) {
+  const double den = g1 * (W * W) - 1.0;
+  const double V = (g1 * (W * W) * (tau + D) - D * W) / den;
+  const double dV = (g1 * W * (D * W - 2.0 * (tau + D)) + D) / (den * den);
+  const double W3 = W * W * W;
+  res = (V * V) * (1.0 - 1.0 / (W * W)) - Q2;
+  dres = 2.0 * V * (dV * (W3 - W) + V) / W3;
+}
+// equations.f90:343-424 (per-call locals reproduce the reference: its SAVE'd d, e are
+// written in the first iteration before being read)
+__device__ double root_brent(double g1, double rho_floor, double D, double tau, double Q2) {
+  const double EPS = 3.0e-8, x_acc = 1.0e-8, x1 = 1.0;
+  const double Wg = (sqrt(Q2) + D) / rmax(D, rho_floor);
+  const double x2 = rmax(1.0e4, Wg * 2.0);
+  double a, b, c, d = 0.0, e = 0.0, fa, fb, fc, o, q, r, y1, tol1, xm, df;
+  residual(g1, x1, D, tau, Q2, fa, df);
+  residual(g1, x2, D, tau, Q2, fb, df);
+  if (sgn1(fa) * sgn1(fb) > 0.0) return -1.0;
+  a = x1; b = x2; c = b; fc = fb;
+  for (int it = 0; it < 100; ++it) {
+    if (sgn1(fb) * sgn1(fc) > 0.0) { c = a; fc = fa; d = b - a; e = d; }
+    if (fabs(fc) < fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+    tol1 = 2.0 * EPS * fabs(b) + 0.5 * x_acc;
+    xm = 0.5 * (c - b);
+    if (fabs(xm) <= tol1 || fabs(fb) < 1.0e-14) return b;
+    if (fabs(e) >= tol1 && fabs(fa) > fabs(fb)) {
+      y1 = fb / fa;
+      if (fabs(a - c) < 1.0e-14) { o = 2.0 * xm * y1; q = 1.0 - y1; }
+      else {
+        q = fa / fc; r = fb / fc;
+        o = y1 * (2.0 * xm * q * (q - r) - (b - a) * (r - 1.0));
+        q = (q - 1.0) * (r - 1.0) * (y1 - 1.0);
+      }
+      if (o > 0.0) q = -q;
+      o = fabs(o);
+      if (2.0 * o < rmin(3.0 * xm * q - fabs(tol1 * q), fabs(e * q))) { e = d; d = o / q; }
+      else { d = xm; e = d; }
+    } else { d = xm; e = d; }
+    a = b; fa = fb;
+    if (fabs(d) > tol1) b = b + d; else b = b + copysign(tol1, xm);
+    residual(g1, b, D, tau, Q2, fb, df);
+  }
+  return -1.0;
+}
+// equations.f90:249-340
+__device__ double root_safe_newton(double g1, double rho_floor, double D, double tau, double Q2, unsigned &flags) {
+  const double x_acc = 1.0e-10, x1 = 1.0;
+  const double Wg = (sqrt(Q2) + D) / rmax(D, rho_floor);
+  const double x2 = rmax(1.0e3, Wg * 2.0);
+  double x_low = x1, x_high = x2, f_low, f_high, df, f, root, dx, dx_old, tmp;
+  residual(g1, x1, D, tau, Q2, f_low, df);
+  residual(g1, x2, D, tau, Q2, f_high, df);
+  if (fabs(f_low) < 1.0e-14) return x_low;
+  if (fabs(f_high) < 1.0e-14) return x_high;
+  if (sgn1(f_low) * sgn1(f_high) > 0.0) return -1.0;
+  if (f_low < 0.0) { x_low = x1; x_high = x2; } else { x_high = x1; x_low = x2; }
+  root = 0.5 * (x1 + x2);
+  dx_old = fabs(x2 - x1);
+  dx = dx_old;
+  residual(g1, root, D, tau, Q2, f, df);
+  for (int it = 0; it < 100; ++it) {
+    if (((root - x_high) * df - f) * ((root - x_low) * df - f) > 0.0 || fabs(2.0 * f) > fabs(dx_old * df)) {
+      dx_old = dx;
+      dx = 0.5 * (x_high - x_low);
+      root = x_low + dx;
+      if (fabs(x_low - root) < 1.0e-14) return root;
+    } else {
+      dx_old = dx;
+      dx = f / df;
+      tmp = root;
+      root = root - dx;
+      if (fabs(tmp - root) < 1.0e-14) return root;
+    }
+    if (fabs(dx) < x_acc) return root;
+    residual(g1, root, D, tau, Q2, f, df);
+    if (f < 0.0) x_low = root; else x_high = root;
+  }
+  flags |= C2P_BRENT;
+  return root_brent(g1, rho_floor, D, tau, Q2);
+}
+
+// cons_to_prim, equations.f90:94-205: cons modified in place (intent(inout)); returns flags
+__device__ unsigned cons_to_prim(const Phys &P, const CellMetric &m, double (&cs)[NEQ], double (&pr)[NEQ]) {
+  unsigned flags = 0;
+  const double lDf = P.rho_floor * m.sqg;
+  const double lTf = P.p_floor * (P.g1 - 1.0) * m.sqg;
+  bool floor_state = false;
+  if (cs[EQ_DE] <= lDf) {
+    flags |= C2P_FLOOR_PRE;
+    floor_state = true;
+  } else {
+    const double S1 = cs[EQ_VX], S2 = cs[EQ_VY], S3 = cs[EQ_VZ];
+    const double S_sq = S1 * (m.i11 * S1 + m.i12 * S2 + m.i13 * S3) + S2 * (m.i12 * S1 + m.i22 * S2 + m.i23 * S3) +
+                        S3 * (m.i13 * S1 + m.i23 * S2 + m.i33 * S3);
+    const double E = cs[EQ_PR] + cs[EQ_DE];
+    const double S_sq_max = rmax(0.0, E * E - cs[EQ_DE] * cs[EQ_DE]) * P.v_max;
+    if (S_sq > S_sq_max && S_sq > 1.0e-20) {
+      flags |= C2P_CAUSAL;
+      const double sf = sqrt(S_sq_max / S_sq);
+      cs[EQ_VX] = cs[EQ_VX] * sf;
+      cs[EQ_VY] = cs[EQ_VY] * sf;
+      cs[EQ_VZ] = cs[EQ_VZ] * sf;
+    }
+    const double D = cs[EQ_DE], tau = cs[EQ_PR];
+    const double Q2 = qsq(m, cs[EQ_VX], cs[EQ_VY], cs[EQ_VZ]);
+    const double W = root_safe_newton(P.g1, P.rho_floor, D, tau, Q2, flags);
+    if (W < 1.0) {
+      flags |= C2P_ROOT_FAIL;
+      floor_state = true;
+    } else {
+      const double den = P.g1 * (W * W) - 1.0;
+      const double V = (P.g1 * (W * W) * (tau + D) - D * W) / den;
+      if (V <= 0.0 || isnan(V)) {
+        flags |= C2P_BAD_V;
+        floor_state = true;
+      } else {
+        const double s1 = cs[EQ_VX], s2 = cs[EQ_VY], s3 = cs[EQ_VZ];
+        pr[EQ_DE] = D / (W * m.sqg);
+        pr[EQ_PR] = (V - tau - D) / m.sqg;
+        pr[EQ_VX] = (m.i11 * s1 + m.i12 * s2 + m.i13 * s3) / V;
+        pr[EQ_VY] = (m.i12 * s1 + m.i22 * s2 + m.i23 * s3) / V;
+        pr[EQ_VZ] = (m.i13 * s1 + m.i23 * s2 + m.i33 * s3) / V;
+        const double a = pr[EQ_VX], b = pr[EQ_VY], c = pr[EQ_VZ];
+        double vsf = 0.0;
+        vsf = vsf + m.g11 * a * a; vsf = vsf + m.g12 * a * b; vsf = vsf + m.g13 * a * c;
+        vsf = vsf + m.g12 * b * a; vsf = vsf + m.g22 * b * b; vsf = vsf + m.g23 * b * c;
+        vsf = vsf + m.g13 * c * a; vsf = vsf + m.g23 * c * b; vsf = vsf + m.g33 * c * c;
+        if (pr[EQ_DE] < P.rho_floor || pr[EQ_PR] < P.p_floor || isnan(pr[EQ_DE]) || isnan(pr[EQ_PR]) ||
+            isnan(a) || isnan(b) || isnan(c) || isnan(vsf) || vsf >= P.v_max) {
+          flags |= C2P_SANITISE;
+          floor_state = true;
+        }
+      }
+    }
+  }
+  if (floor_state) {
+    pr[EQ_DE] = P.rho_floor; pr[EQ_PR] = P.p_floor; pr[EQ_VX] = 0.0; pr[EQ_VY] = 0.0; pr[EQ_VZ] = 0.0;
+    cs[EQ_DE] = lDf; cs[EQ_PR] = lTf; cs[EQ_VX] = 0.0; cs[EQ_VY] = 0.0; cs[EQ_VZ] = 0.0;
+  }
+  return flags;
+}
+
+// prim_to_cons, equations.f90:30-88 (FP64)
+__device__ __forceinline__ void prim_to_cons(const Phys &P, const CellMetric &m, const double (&q)[NEQ], double (&u)[NEQ]) {
+  FaceMetric<double> fm;
+  fm.g11 = m.g11; fm.g12 = m.g12; fm.g13 = m.g13; fm.g22 = m.g22; fm.g23 = m.g23; fm.g33 = m.g33;
+  double v[3] = {q[EQ_VX], q[EQ_VY], q[EQ_VZ]}, vc[3];
+  const double vsq = cap_velocity(fm, v, P.v_max);
+  lower(fm, v, vc);
+  const double h = 1.0 + P.g1 * q[EQ_PR] / q[EQ_DE];
+  const double W = 1.0 / sqrt(1.0 - vsq);
+  const double rhW2 = q[EQ_DE] * h * (W * W);
+  u[EQ_DE] = q[EQ_DE] * W;
+  u[EQ_PR] = rhW2 - q[EQ_PR] - q[EQ_DE] * W;
+  u[EQ_VX] = rhW2 * vc[0];
+  u[EQ_VY] = rhW2 * vc[1];
+  u[EQ_VZ] = rhW2 * vc[2];
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) u[n] = u[n] * m.sqg;
+}
+
+}  // namespace grhd

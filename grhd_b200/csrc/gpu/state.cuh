@@ -1,0 +1,184 @@
+// state.cuh -- device layout of one grid and the boundary fill evaluated on load.
+//
+// Primitives are stored for interior cells only, structure-of-arrays: plane v holds
+// p(v, 1:nx, 1:ny, 1:nz) with i fastest.  Ghost cells are never stored: a stencil load
+// that leaves the domain along one direction returns the value set_boundary_conditions
+// (conditions.f90:773-1066) would have written there.  calc_rhs reads only ghost cells
+// that are outside the domain in exactly one direction (its strips, evolution.f90:60,
+// :112, :164, run through interior cells), and each such ghost is a function of one
+// interior cell plus static data, so evaluating it on load is exact.
+//
+// One ghost index is never written by the reference's boundary routines: -nghost (the
+// loops fill 1-g for g = 1..nghost).  It keeps whatever the caller's array held when the
+// state was uploaded (the jet case re-initialises it to the ambient state every call,
+// conditions.f90:824-835).  Only the shock sensor of nghost = 2 schemes reads it
+// (reconstruction.f90:334-341 at face 0); those values are kept in "frozen" slabs.
+#pragma once
+
+#include "physics.cuh"
+
+namespace grhd {
+
+// centre table fields (per (i,j); the metric cache is k-invariant)
+enum CentreField {
+  CF_ALPHA = 0, CF_B1, CF_B2, CF_B3,
+  CF_G11, CF_G12, CF_G13, CF_G22, CF_G23, CF_G33,
+  CF_I11, CF_I12, CF_I13, CF_I22, CF_I23, CF_I33,
+  CF_SQG,
+  CF_GM = 17,    // g^{mu nu}, 10 symmetric entries
+  CF_CH0 = 27,   // Gamma^0_{mu nu}, 10 symmetric entries
+  CF_DG = 37,    // d_d g_{mu nu}, d = 1..3, 10 symmetric entries each
+  CF_DLNA = 67,  // d_mu ln(alpha), 4 entries
+  CF_VA = 71,    // beta^1 / alpha (shift-aware outflow clamp, conditions.f90:926)
+  NCF = 72
+};
+// face table fields (per face of one direction)
+enum FaceField {
+  FF_ALPHA = 0, FF_BETA_N, FF_G11, FF_G12, FF_G13, FF_G22, FF_G23, FF_G33, FF_SQG, FF_GUP,
+  FF_COF = 10,  // coframe(a,i) at FF_COF + 3a + i
+  FF_FRAME_OK = 19, FF_ZERO = 20, NFF = 21
+};
+
+__host__ __device__ __forceinline__ int sym4(int mu, int nu) {
+  if (mu > nu) { int t = mu; mu = nu; nu = t; }
+  // 00 01 02 03 11 12 13 22 23 33
+  return mu == 0 ? nu : (mu == 1 ? 3 + nu : (mu == 2 ? 5 + nu : 9));
+}
+
+struct GridDev {
+  // sizes
+  int nx, ny, nz, ng;
+  int case_id;
+  long long ncell;   // nx*ny*nz
+  long long pplane;  // plane stride of the primitive / conserved arrays (elements)
+  // metric tables
+  const double *centre;  // [NCF][nij]
+  long long nij;
+  const double *face[3];  // [NFF][nface_d]
+  long long nface[3];
+  // boundary data
+  const double *inj;     // Michel injector [v][g][j][k]  (5*g*ny*nz)
+  const double *dust;    // [v][g]
+  const double *xc;      // x(-g:nx+g)
+  const double *frozen[3];  // -nghost slabs [v][..] (nghost == 2 only)
+  double jet[7];
+  double rho_floor, p_floor;
+};
+
+// interior primitive read (1-based cell indices)
+template <class PT>
+__device__ __forceinline__ double ld_prim(const PT *__restrict__ P, const GridDev &G, int v, int i, int j, int k) {
+  const long long c = (long long)(i - 1) + (long long)G.nx * ((long long)(j - 1) + (long long)G.ny * (k - 1));
+  return (double)__ldg(&P[v * G.pplane + c]);
+}
+template <class PT>
+__device__ __forceinline__ void ld_cell(const PT *__restrict__ P, const GridDev &G, int i, int j, int k, double (&q)[NEQ]) {
+  const long long c = (long long)(i - 1) + (long long)G.nx * ((long long)(j - 1) + (long long)G.ny * (k - 1));
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) q[v] = (double)__ldg(&P[v * G.pplane + c]);
+}
+__device__ __forceinline__ int wrap(int i, int n) {  // periodic (whole-array statements per g) == modular
+  int r = (i - 1) % n;
+  if (r < 0) r += n;
+  return r + 1;
+}
+__device__ __forceinline__ void jet_ambient(const GridDev &G, double (&q)[NEQ]) {
+  q[EQ_DE] = G.jet[0]; q[EQ_PR] = G.jet[1]; q[EQ_VX] = 0.0; q[EQ_VY] = 0.0; q[EQ_VZ] = G.jet[2];
+}
+
+// Value of cell (i,j,k) where only the DIR index may lie outside [1, n_DIR].
+template <int DIR, class PT>
+__device__ __forceinline__ void load_cell(const PT *__restrict__ P, const GridDev &G, int i, int j, int k, double (&q)[NEQ]) {
+  const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
+  const int idx = DIR == 1 ? i : (DIR == 2 ? j : k);
+  if (idx >= 1 && idx <= n) { ld_cell(P, G, i, j, k, q); return; }
+  const int cs = G.case_id;
+  if (idx == -G.ng) {  // never written by the boundary loops (see header)
+    if (cs == 5) { jet_ambient(G, q); return; }
+    const double *fz = G.frozen[DIR - 1];
+    long long s, ns;
+    if (DIR == 1) { s = (j - 1) + (long long)G.ny * (k - 1); ns = (long long)G.ny * G.nz; }
+    else if (DIR == 2) { s = (i - 1) + (long long)G.nx * (k - 1); ns = (long long)G.nx * G.nz; }
+    else { s = (i - 1) + (long long)G.nx * (j - 1); ns = (long long)G.nx * G.ny; }
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) q[v] = fz[v * ns + s];
+    return;
+  }
+  const bool lo = idx < 1;
+  const int g = lo ? 1 - idx : idx - n;
+  if (DIR == 1) {
+    switch (cs) {
+      case 1: case 2: case 3:  // zero-gradient outflow, conditions.f90:795-798
+        ld_cell(P, G, lo ? 1 : G.nx, j, k, q); return;
+      case 4: case 6:  // periodic, conditions.f90:809-811
+        ld_cell(P, G, wrap(i, G.nx), j, k, q); return;
+      case 5:  // reflecting axis / ambient, conditions.f90:838-848
+        if (lo) { ld_cell(P, G, g, j, k, q); q[EQ_VX] = -q[EQ_VX]; } else jet_ambient(G, q);
+        return;
+      case 7:  // copy inside, analytic injector outside, conditions.f90:872-883
+        if (lo) ld_cell(P, G, 1, j, k, q);
+        else {
+#pragma unroll
+          for (int v = 0; v < NEQ; ++v)
+            q[v] = G.inj[(long long)v * G.ng * G.ny * G.nz + (g - 1) + (long long)G.ng * ((j - 1) + (long long)G.ny * (k - 1))];
+        }
+        return;
+      case 8:  // dust, conditions.f90:896-907
+        if (lo) {
+          ld_cell(P, G, 1, j, k, q);
+          q[EQ_DE] = rmax(q[EQ_DE], G.rho_floor);
+          q[EQ_PR] = rmax(q[EQ_PR], G.p_floor);
+          q[EQ_VX] = rmin(0.0, q[EQ_VX]);
+        } else {
+#pragma unroll
+          for (int v = 0; v < NEQ; ++v) q[v] = G.dust[v * G.ng + (g - 1)];
+        }
+        return;
+      default: {  // 9-12: shift-aware radial outflow, conditions.f90:916-938, :951-973, :1007-1026
+        const int src = lo ? 1 : G.nx;
+        ld_cell(P, G, src, j, k, q);
+        const double d_in = q[EQ_DE];
+        const double va = G.centre[(long long)CF_VA * G.nij + (src - 1) + (long long)G.nx * (j - 1)];
+        q[EQ_DE] = rmax(q[EQ_DE], G.rho_floor);
+        q[EQ_PR] = rmax(q[EQ_PR], G.p_floor);
+        q[EQ_VX] = lo ? rmin(va, q[EQ_VX]) : rmax(va, q[EQ_VX]);
+        if (lo && (cs == 9 || cs == 10) && d_in < 1.0e-6) { q[EQ_VY] = 0.0; q[EQ_VZ] = 0.0; }
+        return;
+      }
+    }
+  } else if (DIR == 2) {
+    if (cs == 5) { jet_ambient(G, q); return; }  // reset to ambient, no y fill (conditions.f90:824-835)
+    if (cs == 11) {  // reflecting poles, conditions.f90:977-988 (ny >= nghost enforced)
+      ld_cell(P, G, i, lo ? g : G.ny + 1 - g, k, q);
+      q[EQ_VY] = -q[EQ_VY];
+      return;
+    }
+    if (cs == 12) {  // trans-polar, conditions.f90:1033-1050 (ny >= nghost, nz even enforced)
+      int ks = k + G.nz / 2;
+      if (ks > G.nz) ks -= G.nz;
+      ld_cell(P, G, i, lo ? g : G.ny + 1 - g, ks, q);
+      q[EQ_VY] = -q[EQ_VY];
+      return;
+    }
+    ld_cell(P, G, i, wrap(j, G.ny), k, q);  // periodic
+    return;
+  } else {
+    if (cs == 5) {  // nozzle inflow / reflecting wall below, outflow above, conditions.f90:851-869
+      if (lo) {
+        if (G.xc[i + G.ng] <= G.jet[3]) {
+          q[EQ_DE] = G.jet[4]; q[EQ_PR] = G.jet[5]; q[EQ_VX] = 0.0; q[EQ_VY] = 0.0; q[EQ_VZ] = G.jet[6];
+        } else {
+          ld_cell(P, G, i, j, g, q);
+          q[EQ_VZ] = -q[EQ_VZ];
+        }
+      } else {
+        ld_cell(P, G, i, j, G.nz, q);
+        q[EQ_VZ] = rmax(0.0, q[EQ_VZ]);
+      }
+      return;
+    }
+    ld_cell(P, G, i, j, wrap(k, G.nz), q);  // periodic
+  }
+}
+
+}  // namespace grhd

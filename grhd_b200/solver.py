@@ -1,0 +1,169 @@
+"""Python front end of the drop-in boundary (include/grhd2_gpu.h).
+
+:class:`GpuGrid` owns one ``grhd2_gpu`` handle: the device-resident state of one grid and
+the per-stage kernels.  It mirrors the module-level surface of the reference that the
+C-ABI replaces -- ``calc_rhs``, ``update_adaptive_dt``, ``cons_to_prim``, ``prim_to_cons``,
+``set_boundary_conditions`` and the SSP-RK3 step of grhd2.f90 -- with the same argument
+meaning, layouts and error behaviour (a nonzero status raises :class:`GpuError` carrying
+the library's message).  There is no CPU fallback: a missing library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native as N
+from .problem import Problem
+
+PRECISION = {"fp64": 0, "mixed": 1}
+
+
+class GpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"grhd2_gpu error {code}: {msg}")
+        self.code = code
+
+
+class GpuGrid:
+    """One grid on the GPU, built from a :class:`Problem` (or explicit config/tables)."""
+
+    def __init__(self, problem: Problem, precision: str = "fp64", upload_initial: bool = True):
+        self.lib = N.gpu_lib()
+        self.problem = problem
+        self.precision = precision
+        self.cfg = problem.config(PRECISION[precision])
+        self._mv = problem.metric_view()
+        self._bv = problem.bc_view()
+        h = C.c_void_p()
+        rc = self.lib.grhd2_gpu_create(C.byref(self.cfg), C.byref(h))
+        self._h = h
+        self._check(rc)
+        self._check(self.lib.grhd2_gpu_set_metric(self._h, C.byref(self._mv)))
+        self._check(self.lib.grhd2_gpu_set_bc_data(self._h, C.byref(self._bv)))
+        if upload_initial:
+            p0 = problem.initial_prims()
+            self.upload(p=p0)
+            self.prim_to_cons()
+
+    # ---- plumbing ------------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self.lib.grhd2_gpu_last_error(self._h) if self._h else b"create failed"
+            raise GpuError(rc, (msg or b"").decode())
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.grhd2_gpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- the reference surface -------------------------------------------------------
+    def upload(self, up: np.ndarray | None = None, p: np.ndarray | None = None):
+        if up is not None:
+            up = np.ascontiguousarray(up, dtype=np.float64)
+            assert up.size == 5 * self.problem.n_cells
+        if p is not None:
+            p = np.ascontiguousarray(p, dtype=np.float64)
+            assert p.shape == self.problem.prim_shape
+        self._check(self.lib.grhd2_gpu_upload(self._h, N.dptr(up), N.dptr(p)))
+
+    def prim_to_cons(self):
+        """up = prim_to_cons(p) over interior cells (grhd2.f90:126-134)."""
+        self._check(self.lib.grhd2_gpu_prim_to_cons_all(self._h))
+
+    def cons_to_prim(self):
+        """p = cons_to_prim(up), up floored in place (grhd2.f90:252-260)."""
+        self._check(self.lib.grhd2_gpu_cons_to_prim_all(self._h))
+
+    def set_boundary(self):
+        self._check(self.lib.grhd2_gpu_set_boundary(self._h))
+
+    def cfl(self) -> float:
+        """dt of update_adaptive_dt (evolution.f90:198)."""
+        dt = C.c_double()
+        self._check(self.lib.grhd2_gpu_cfl(self._h, C.byref(dt)))
+        return dt.value
+
+    def step(self, dt: float):
+        """One SSP-RK3 step (grhd2.f90:232-265), asynchronous on the handle's stream."""
+        self._check(self.lib.grhd2_gpu_step(self._h, dt))
+
+    def run(self, t0: float, final_time: float, max_steps: int = -1):
+        """Time loop of grhd2.f90:179-265 without I/O; returns (steps, t)."""
+        t = C.c_double()
+        n = C.c_int64()
+        self._check(self.lib.grhd2_gpu_run(self._h, t0, final_time, max_steps, C.byref(t), C.byref(n)))
+        return n.value, t.value
+
+    def calc_rhs(self) -> np.ndarray:
+        """calc_rhs(p) of the resident primitives (evolution.f90:30), (5,nx,ny,nz) layout."""
+        rhs = np.empty(self.problem.cons_shape)
+        self._check(self.lib.grhd2_gpu_calc_rhs(self._h, N.dptr(rhs)))
+        return rhs
+
+    def download(self, p_template: np.ndarray | None = None):
+        """(up, p): p holds interior cells and single-direction ghosts; the remaining
+        ghost entries keep the values of p_template (zeros by default)."""
+        up = np.empty(self.problem.cons_shape)
+        p = np.zeros(self.problem.prim_shape) if p_template is None else np.array(p_template, dtype=np.float64)
+        self._check(self.lib.grhd2_gpu_download(self._h, N.dptr(up), N.dptr(p)))
+        return up, p
+
+    def counters(self) -> dict:
+        c = N.Counters()
+        self._check(self.lib.grhd2_gpu_get_counters(self._h, C.byref(c)))
+        return c.as_dict()
+
+    def reset_counters(self):
+        self._check(self.lib.grhd2_gpu_reset_counters(self._h))
+
+    def synchronize(self):
+        self._check(self.lib.grhd2_gpu_synchronize(self._h))
+
+    # ---- single-face entry points ------------------------------------------------------
+    def riemann_faces(self, dir: int, qL, qR, alpha, beta, gamma, sqg) -> np.ndarray:
+        """resolve_riemann_problem (fluxes.f90:56) for n independent faces.
+        qL, qR: (n,5); alpha, sqg: (n,); beta: (n,3); gamma: (n,3,3) (symmetric)."""
+        qL, qR = (np.ascontiguousarray(a, dtype=np.float64) for a in (qL, qR))
+        n = qL.shape[0]
+        alpha, sqg = (np.ascontiguousarray(np.broadcast_to(a, (n,)), dtype=np.float64) for a in (alpha, sqg))
+        beta = np.ascontiguousarray(np.broadcast_to(beta, (n, 3)), dtype=np.float64)
+        # Fortran (3,3) order per face: g[(a-1)+3(b-1)] -> transpose of a C (3,3)
+        gamma = np.ascontiguousarray(np.broadcast_to(gamma, (n, 3, 3)).transpose(0, 2, 1), dtype=np.float64)
+        flux = np.empty((n, 5))
+        self._check(self.lib.grhd2_gpu_riemann_faces(self._h, n, dir, N.dptr(qL), N.dptr(qR), N.dptr(alpha),
+                                                     N.dptr(beta), N.dptr(gamma), N.dptr(sqg), N.dptr(flux)))
+        return flux
+
+    def physical_flux(self, dir: int, q, alpha, beta, gamma, sqg) -> np.ndarray:
+        """calc_fluxes (equations.f90:434) for n states."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        n = q.shape[0]
+        alpha, sqg = (np.ascontiguousarray(np.broadcast_to(a, (n,)), dtype=np.float64) for a in (alpha, sqg))
+        beta = np.ascontiguousarray(np.broadcast_to(beta, (n, 3)), dtype=np.float64)
+        gamma = np.ascontiguousarray(np.broadcast_to(gamma, (n, 3, 3)).transpose(0, 2, 1), dtype=np.float64)
+        flux = np.empty((n, 5))
+        self._check(self.lib.grhd2_gpu_physical_flux(self._h, n, dir, N.dptr(q), N.dptr(alpha), N.dptr(beta),
+                                                     N.dptr(gamma), N.dptr(sqg), N.dptr(flux)))
+        return flux
+
+
+def l1_relative(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Per-variable sum|a-b| / sum|b| over interior cells; arrays in (…,5) layout."""
+    a = a.reshape(-1, 5)
+    b = b.reshape(-1, 5)
+    den = np.abs(b).sum(axis=0)
+    num = np.abs(a - b).sum(axis=0)
+    return np.where(den > 0, num / np.where(den > 0, den, 1.0), num)

@@ -1,0 +1,158 @@
+/*
+ * grhd2_gpu.h -- C-ABI of the B200 replacement for GRHD2's per-stage RHS and update path.
+ *
+ * The Fortran driver (grhd2.f90) keeps its .par parser, I/O and diagnostics and calls
+ * these entry points through ISO_C_BINDING in place of the module procedures named in
+ * each comment (file:line in RuelasF/GRHD).  All arguments are plain C types; every array
+ * is in the reference's own Fortran layout (column-major, neq=5 fastest), so the Fortran
+ * side passes c_loc() of its module arrays unchanged.
+ *
+ * Ownership: the caller owns host arrays; the library copies in and out.  The library owns
+ * all device memory and one CUDA stream per handle.  State stays resident on the device
+ * between calls; download() is only needed before output, checkpoints and diagnostics.
+ *
+ * Errors: every int-returning entry point returns 0 on success and a negative code on
+ * failure; grhd2_gpu_last_error() gives the message.  The Fortran shim turns a nonzero
+ * status into "write(*,*) msg; error stop 1", the reference's own convention
+ * (evolution.f90:214-215, parameters.f90:1085-1096).
+ *
+ * Threading: one handle is used by one host thread at a time; handles are independent.
+ */
+#ifndef GRHD2_GPU_H
+#define GRHD2_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRHD2_GPU_ABI_VERSION 1
+
+/* error codes */
+#define GRHD2_OK 0
+#define GRHD2_ERR_ARG -1      /* invalid argument or configuration */
+#define GRHD2_ERR_CUDA -2     /* CUDA runtime error (no device, launch failure, ...) */
+#define GRHD2_ERR_NOMEM -3    /* device allocation failed */
+#define GRHD2_ERR_STATE -4    /* call out of order (e.g. step before set_metric) */
+#define GRHD2_ERR_CFL -5      /* non-finite metric or spacing in the CFL (evolution.f90:257-272) */
+#define GRHD2_ERR_BOUNDARY -6 /* boundary precondition (e.g. nz odd for the 3D torus, conditions.f90:999) */
+
+/* identifiers: variables.f90:224-243 */
+enum { GRHD2_REC_GODUNOV = 1, GRHD2_REC_TVD = 2, GRHD2_REC_WENO3 = 3, GRHD2_REC_MP5 = 4,
+       GRHD2_REC_WENO5 = 5 };
+enum { GRHD2_RS_HLLE = 1, GRHD2_RS_HLLC = 2 };
+enum { GRHD2_LIM_MINMOD = 1, GRHD2_LIM_SUPERBEE = 2, GRHD2_LIM_MC = 3 };
+/* metric_type / geom_type strings of variables.f90:129-133 as integers */
+enum { GRHD2_METRIC_MINKOWSKI = 0, GRHD2_METRIC_EF = 1, GRHD2_METRIC_KS = 2 };
+enum { GRHD2_GEOM_CARTESIAN = 0, GRHD2_GEOM_CYLINDRICAL = 1, GRHD2_GEOM_SPHERICAL = 2,
+       GRHD2_GEOM_SPHEROIDAL = 3 };
+/* precision policies */
+enum { GRHD2_PREC_FP64 = 0, GRHD2_PREC_MIXED = 1 };
+
+/* Filled by the Fortran side from the globals of variables.f90.  case_id selects the
+ * boundary routine of conditions.f90:773 (1 Sod, 2 strong shock, 3 Shu-Osher, 4 KHI,
+ * 5 jet, 6 convergence, 7 Michel, 8 dust, 9 off-axis, 10 FM equatorial, 11 FM sagittal,
+ * 12 FM 3D). */
+typedef struct {
+  int32_t nx, ny, nz, nghost, neq;                         /* neq must be 5 */
+  int32_t rec_method, tvd_limiter, riemann, shock_sensor;  /* REC_*, LIM_*, RS_*, 0/1 */
+  int32_t metric_kind, geom_kind, use_log_r, case_id;
+  int32_t precision_policy;                                /* GRHD2_PREC_* */
+  int32_t reserved;
+  double dx, dy, dz, adb_idx, g1, cfl;
+  double rho_floor, p_floor, v_max;                        /* 1e-10, 1e-13, 1-1e-5 */
+} grhd2_gpu_config;
+
+/* The k = 1 slices (the cache is k-invariant: initialization.f90:283,331,351,379) of the
+ * reference's metric cache, variables.f90:70-99, Fortran order. */
+typedef struct {
+  const double *alpha_c;      /* (nx,ny)            */
+  const double *beta_c;       /* (3,nx,ny)          */
+  const double *gamma_c;      /* (3,3,nx,ny)        */
+  const double *gamma_inv_c;  /* (3,3,nx,ny)        */
+  const double *gmunu_c;      /* (0:3,0:3,nx,ny)    */
+  const double *sqrt_gamma_c; /* (nx,ny)            */
+  const double *chris_c;      /* (0:3,0:3,0:3,nx,ny)*/
+  const double *dg_c;         /* (0:3,0:3,1:3,nx,ny)*/
+  const double *dlna_c;       /* (0:3,nx,ny)        */
+  const double *alpha_f_x, *beta_f_x, *gamma_f_x, *sqrt_gamma_f_x; /* (..,nx+1,ny), may be NULL if nx==1 */
+  const double *alpha_f_y, *beta_f_y, *gamma_f_y, *sqrt_gamma_f_y; /* (..,nx,ny+1), NULL if ny==1 */
+  const double *alpha_f_z, *beta_f_z, *gamma_f_z, *sqrt_gamma_f_z; /* (..,nx,ny),   NULL if nz==1 */
+  const double *x_face;       /* (0:nx)  cylindrical axis test, evolution.f90:69 */
+  const double *y_face;       /* (0:ny)  polar-face test, evolution.f90:122      */
+} grhd2_gpu_metric_view;
+
+/* Per-case boundary data (conditions.f90:229-246, :249-278, :820-870). */
+typedef struct {
+  const double *michel_injector; /* (5,nghost,ny,nz), case 7, else NULL */
+  const double *dust_outer;      /* (5,nghost): evaluate_dust_accretion_state(x(nx+g)), case 8 */
+  const double *x_c;             /* x(-g:nx+g) cell centres, case 5 nozzle test */
+  double jet[7];                 /* ambient rho, p, vz; nozzle radius; jet rho, p, vz */
+} grhd2_gpu_bc_view;
+
+/* Failure and floor counters.  The reference keeps none; these count the branches of
+ * cons_to_prim (equations.f90:116-204), the reconstruction floors
+ * (reconstruction.f90:647-654) and HLLC exits to HLLE (fluxes.f90:195-396). */
+typedef struct {
+  int64_t c2p_floor_pre, c2p_causal_rescale, c2p_brent_used, c2p_root_fail, c2p_bad_V,
+          c2p_final_sanitise, recon_floor_clamps, hllc_fallbacks;
+} grhd2_gpu_counters;
+
+typedef struct grhd2_gpu grhd2_gpu;
+
+/* Create a handle on the current CUDA device (allocates device state).  Replaces the
+ * allocation half of allocate_and_grid (initialization.f90:84) for the hot-path arrays. */
+int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out);
+/* Upload the metric cache tables (precalculate_metric_cache, initialization.f90:265). */
+int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m);
+/* Upload per-case boundary data (cache_michel_injector, conditions.f90:229). */
+int grhd2_gpu_set_bc_data(grhd2_gpu *h, const grhd2_gpu_bc_view *b);
+/* Copy state in: up(5,nx,ny,nz) and/or p(5,-g:nx+g,-g:ny+g,-g:nz+g); either may be NULL.
+ * Used after initialisation, restart (grhd2.f90:95-116) and host-side perturbations. */
+int grhd2_gpu_upload(grhd2_gpu *h, const double *up, const double *p);
+/* up = prim_to_cons(p) over interior cells (grhd2.f90:126-134, equations.f90:30). */
+int grhd2_gpu_prim_to_cons_all(grhd2_gpu *h);
+/* dt = update_adaptive_dt() (evolution.f90:198). */
+int grhd2_gpu_cfl(grhd2_gpu *h, double *dt_out);
+/* One SSP-RK3 step of size dt: u = up; 3 x (rhs, combine, con2prim, boundary)
+ * (grhd2.f90:232-265). */
+int grhd2_gpu_step(grhd2_gpu *h, double dt);
+/* The time loop body of grhd2.f90:179-265 without I/O: steps until t >= final_time or
+ * max_steps steps (max_steps < 0: no limit), clamping the last dt (grhd2.f90:182-184). */
+int grhd2_gpu_run(grhd2_gpu *h, double t0, double final_time, int64_t max_steps,
+                  double *t_out, int64_t *steps_out);
+/* rhs(5,nx,ny,nz) = calc_rhs(p) of the resident primitives (evolution.f90:30). */
+int grhd2_gpu_calc_rhs(grhd2_gpu *h, double *rhs_host);
+/* p = cons_to_prim(up) over interior cells, up modified in place (grhd2.f90:252-260). */
+int grhd2_gpu_cons_to_prim_all(grhd2_gpu *h);
+/* set_boundary_conditions(p) (conditions.f90:773).  The device state holds no ghost
+ * cells (they are evaluated on load), so this only checks the case preconditions. */
+int grhd2_gpu_set_boundary(grhd2_gpu *h);
+/* Copy state out; either pointer may be NULL.  p receives interior cells and every ghost
+ * cell that lies outside the domain in exactly one direction, filled as
+ * set_boundary_conditions fills it; ghost cells outside in two or more directions
+ * (never read by calc_rhs) are left untouched in the caller's array. */
+int grhd2_gpu_download(grhd2_gpu *h, double *up, double *p);
+int grhd2_gpu_get_counters(grhd2_gpu *h, grhd2_gpu_counters *out);
+int grhd2_gpu_reset_counters(grhd2_gpu *h);
+/* Face fluxes for n independent faces (resolve_riemann_problem, fluxes.f90:56):
+ * qL,qR,flux (5,n); alpha,sqg (n); beta (3,n); gamma (3,3,n); dir 1..3.  Uses the
+ * handle's physics settings (riemann, adb_idx, metric/geometry kind). */
+int grhd2_gpu_riemann_faces(grhd2_gpu *h, int n, int dir, const double *qL, const double *qR,
+                            const double *alpha, const double *beta, const double *gamma,
+                            const double *sqg, double *flux);
+/* Physical flux F(q) for n states (calc_fluxes, equations.f90:434). */
+int grhd2_gpu_physical_flux(grhd2_gpu *h, int n, int dir, const double *q, const double *alpha,
+                            const double *beta, const double *gamma, const double *sqg,
+                            double *flux);
+/* Wait for all work of the handle; returns the first asynchronous error. */
+int grhd2_gpu_synchronize(grhd2_gpu *h);
+const char *grhd2_gpu_last_error(const grhd2_gpu *h);
+void grhd2_gpu_destroy(grhd2_gpu *h);
+int grhd2_gpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,68 @@
+/*
+ * grhd2_host.h -- host-side problem setup that feeds the grhd2_gpu C-ABI.
+ *
+ * In a Fortran deployment this side is the unchanged reference driver: the .par reader
+ * (parameters.f90), the presets and the metric cache (initialization.f90), the initial
+ * conditions and perturbations (conditions.f90) and the analytic metrics (metrics.f90).
+ * This library restates those init-time routines in C++ so the GPU path can be driven
+ * without a Fortran compiler (benchmarks, the solve server, tests).  It performs no
+ * hot-path arithmetic: every per-stage operation lives in grhd2_gpu.
+ *
+ * Parameters use the reference's .par keys (parameters.f90:147-349), one "key = value"
+ * per line, '#' or '!' comments.  Angles theta_min/max and phi_min/max are in units of pi.
+ */
+#ifndef GRHD2_HOST_H
+#define GRHD2_HOST_H
+
+#include <stdint.h>
+#include "grhd2_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct grhd2_problem grhd2_problem;
+
+typedef struct {
+  int32_t case_id, nx, ny, nz, nghost;
+  int32_t perturbation_type; /* 0 none, 1 pressure noise, 2 density noise, 3 density mode */
+  int64_t perturbation_seed;
+  double final_time, cfl, perturbation_time, perturbation_amplitude, perturbation_mode;
+  double x_min, x_max, y_min, y_max, z_min, z_max;
+  double bh_mass, a_spin, fm_l, fm_w_in;
+} grhd2_problem_info;
+
+/* Build a problem from .par text (problem = sod | michel | fishbone_equatorial | ...). On
+ * failure returns a negative code and writes a message into err (if errlen > 0). */
+int grhd2_problem_create(const char *par_text, grhd2_problem **out, char *err, int errlen);
+void grhd2_problem_destroy(grhd2_problem *pb);
+int grhd2_problem_config(const grhd2_problem *pb, int32_t precision_policy, grhd2_gpu_config *cfg);
+int grhd2_problem_metric(const grhd2_problem *pb, grhd2_gpu_metric_view *mv);
+int grhd2_problem_bc(const grhd2_problem *pb, grhd2_gpu_bc_view *bv);
+int grhd2_problem_info_get(const grhd2_problem *pb, grhd2_problem_info *info);
+/* Initial primitives p(5,-g:nx+g,-g:ny+g,-g:nz+g) after set_initial_conditions
+ * (conditions.f90:26); the array is owned by the problem. */
+const double *grhd2_problem_prims(const grhd2_problem *pb);
+/* Number of doubles in the ghosted primitive array and in an interior conserved array. */
+int64_t grhd2_problem_prim_size(const grhd2_problem *pb);
+int64_t grhd2_problem_cons_size(const grhd2_problem *pb);
+/* Apply the configured perturbation (inject_pressure_noise / inject_density_noise /
+ * inject_density_mode, conditions.f90:603-768) to a ghosted primitive array in place.
+ * The noise generator is SplitMix64(seed) mapped to [0,1), not gfortran's
+ * random_number; the selection rule and the arithmetic are the reference's. */
+int grhd2_problem_perturb(const grhd2_problem *pb, double *p);
+/* Cell-centre coordinates x(-g:nx+g), y(-g:ny+g), z(-g:nz+g). */
+const double *grhd2_problem_x(const grhd2_problem *pb);
+const double *grhd2_problem_y(const grhd2_problem *pb);
+const double *grhd2_problem_z(const grhd2_problem *pb);
+
+/* Analytic metric evaluation at (x, y) for the problem's metric and geometry
+ * (metrics.f90 calculate_metric / christoffel / derivatives); any output may be NULL. */
+int grhd2_problem_eval_metric(const grhd2_problem *pb, double x, double y, double *alpha,
+                              double *beta, double *gamma, double *gmunu, double *det,
+                              double *dlnalpha, double *chris, double *dg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

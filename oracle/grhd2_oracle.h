@@ -1,0 +1,113 @@
+/*
+ * grhd2_oracle.h -- CPU restatement of GRHD2's per-stage RHS and update path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the parity oracle: a plain-C restatement of the
+ * reference Fortran (RuelasF/GRHD) hot path, kept in the reference's own data layout
+ * (Fortran column-major, array-of-structures, neq=5 fastest, ghosted primitives).
+ * Only the test suite, the smoke check and the CPU-baseline leg of the benchmark load it.
+ * The product library never links or calls it.
+ *
+ * Arithmetic follows the reference operation by operation (same evaluation order,
+ * integer powers as repeated products, no FMA contraction: build with
+ * -ffp-contract=off).  Two documented choices where Fortran is processor dependent:
+ *   - MAX/MIN with a NaN argument: sequential "keep the first non-NaN" semantics
+ *     (m = a; if (b > m || m != m) m = b), also used by the CUDA kernels;
+ *   - transcendental functions: the host C library (the same glibc a gfortran build
+ *     calls).
+ *
+ * Layouts (1-based Fortran indices as in variables.f90:60-99):
+ *   p   (5, -g:nx+g, -g:ny+g, -g:nz+g)     primitives, ghosted
+ *   u/up/rhs (5, nx, ny, nz)               conserved, interior only
+ *   metric tables: the k = 1 slice of the reference's metric cache (it is k-invariant,
+ *   initialization.f90:283,331,351,379), Fortran order with (i,j) trailing.
+ */
+#ifndef GRHD2_ORACLE_H
+#define GRHD2_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* identifiers mirror variables.f90:224-243 */
+enum { ORC_REC_GODUNOV = 1, ORC_REC_TVD = 2, ORC_REC_WENO3 = 3, ORC_REC_MP5 = 4, ORC_REC_WENO5 = 5 };
+enum { ORC_RS_HLLE = 1, ORC_RS_HLLC = 2 };
+enum { ORC_LIM_MINMOD = 1, ORC_LIM_SUPERBEE = 2, ORC_LIM_MC = 3 };
+enum { ORC_METRIC_MINKOWSKI = 0, ORC_METRIC_EF = 1, ORC_METRIC_KS = 2 };
+enum { ORC_GEOM_CARTESIAN = 0, ORC_GEOM_CYLINDRICAL = 1, ORC_GEOM_SPHERICAL = 2,
+       ORC_GEOM_SPHEROIDAL = 3 };
+
+typedef struct {
+  int32_t nx, ny, nz, nghost;
+  int32_t rec_method, tvd_limiter, riemann, shock_sensor;
+  int32_t metric_kind, geom_kind, case_id, pad0;
+  double dx, dy, dz, adb_idx, g1, cfl;
+  double rho_floor, p_floor, v_max;
+} orc_config;
+
+typedef struct {
+  /* cell centres, (.., nx, ny) */
+  const double *alpha_c, *beta_c, *gamma_c, *gamma_inv_c, *gmunu_c, *sqrt_gamma_c;
+  const double *chris_c, *dg_c, *dlna_c;
+  /* x faces (.., nx+1, ny), y faces (.., nx, ny+1), z faces (.., nx, ny) */
+  const double *alpha_fx, *beta_fx, *gamma_fx, *sqg_fx;
+  const double *alpha_fy, *beta_fy, *gamma_fy, *sqg_fy;
+  const double *alpha_fz, *beta_fz, *gamma_fz, *sqg_fz;
+  /* coordinates: x_face(0:nx), y_face(0:ny), x centres (-g:nx+g) */
+  const double *x_face, *y_face, *x_c;
+  /* boundary data: Michel injector (5,g,ny,nz), dust outer states (5,g) */
+  const double *michel_injector, *dust_outer;
+  /* jet parameters: ambient rho,p,vz ; nozzle radius ; jet rho,p,vz */
+  double jet[7];
+} orc_metric;
+
+typedef struct {
+  int64_t c2p_floor_pre, c2p_causal_rescale, c2p_brent_used, c2p_root_fail, c2p_bad_V,
+          c2p_final_sanitise, recon_floor_clamps, hllc_fallbacks;
+} orc_counters;
+
+/* evolution.f90:30 calc_rhs */
+void orc_calc_rhs(const orc_config *c, const orc_metric *m, const double *p, double *rhs,
+                  orc_counters *cnt);
+/* evolution.f90:198 update_adaptive_dt; returns 0 or a negative error code */
+int orc_cfl(const orc_config *c, const orc_metric *m, double *dt_out);
+/* equations.f90:94 cons_to_prim for one cell (i,j 1-based; metric is k-invariant) */
+void orc_cons_to_prim(const orc_config *c, const orc_metric *m, double *cons, double *prim,
+                      int i, int j, orc_counters *cnt);
+/* grhd2.f90:252-260 sweep over all interior cells */
+void orc_cons_to_prim_all(const orc_config *c, const orc_metric *m, double *up, double *p,
+                          orc_counters *cnt);
+/* equations.f90:30 prim_to_cons, one cell */
+void orc_prim_to_cons(const orc_config *c, const orc_metric *m, const double *prim,
+                      double *cons, int i, int j);
+void orc_prim_to_cons_all(const orc_config *c, const orc_metric *m, const double *p,
+                          double *up);
+/* conditions.f90:773 set_boundary_conditions; returns 0 or a negative error code */
+int orc_set_boundary(const orc_config *c, const orc_metric *m, double *p);
+/* fluxes.f90:56 resolve_riemann_problem for one face; g is the Fortran (3,3) array */
+void orc_riemann(const orc_config *c, const double *qL, const double *qR, int dir,
+                 double alpha, const double *beta, const double *g, double sqg,
+                 double *flux, orc_counters *cnt);
+/* equations.f90:434 calc_fluxes */
+void orc_physical_flux(const orc_config *c, const double *q, int dir, double alpha,
+                       const double *beta, const double *g, double sqg, double *f);
+/* reconstruction.f90:285 reconstruct_1d_core on one strip prim(5,-g:n+g) */
+void orc_reconstruct(const orc_config *c, const double *prim, int nodes, int dir,
+                     double *qL, double *qR, orc_counters *cnt);
+/* grhd2.f90:232-265: one SSP-RK3 step (u = up; BC; 3 x (rhs, combine, c2p, BC)).
+ * rhs is scratch of size 5*nx*ny*nz. Returns 0 or a negative error code. */
+int orc_step(const orc_config *c, const orc_metric *m, double *u, double *up, double *p,
+             double *rhs, double dt, orc_counters *cnt);
+/* grhd2.f90:179-265 time loop without I/O: runs while t < final_time or until max_steps
+ * steps; returns the number of steps taken (>= 0) or a negative error code. */
+int64_t orc_run(const orc_config *c, const orc_metric *m, double *up, double *p,
+                double t0, double final_time, int64_t max_steps, double *t_out,
+                orc_counters *cnt);
+/* number of OpenMP threads used by orc_run / orc_step (1 without OpenMP) */
+int orc_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
