@@ -44,6 +44,10 @@ struct grhd2_gpu {
   double dt_cache = 0.0;
   bool dt_valid = false;
   std::string err;
+  // per-launch timing (grhd2_gpu_profile_step): events recorded after every launch
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<const char *> prof_names;
+  bool profiling = false;
 };
 
 namespace {
@@ -78,9 +82,16 @@ inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / 
 
 bool bit_equal(double a, double b) { return std::memcmp(&a, &b, sizeof a) == 0; }
 
-int launch_check(grhd2_gpu *h) {
+int launch_check(grhd2_gpu *h, const char *name = nullptr) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(h, GRHD2_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+  if (h->profiling && name) {
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) return fail(h, GRHD2_ERR_CUDA, "cudaEventCreate failed");
+    cudaEventRecord(ev, h->stream);
+    h->prof_ev.push_back(ev);
+    h->prof_names.push_back(name);
+  }
   return 0;
 }
 
@@ -89,12 +100,18 @@ template <class R, class PT>
 int launch_fluxes(grhd2_gpu *h) {
   const GridDev &G = h->G;
   const PT *P = (const PT *)h->P;
+  int rc;
   k_face_flux<1, R, PT><<<nblocks(G.nface[0] * G.nz, 128), 128, 0, h->stream>>>(G, h->phys, P, (R *)h->F[0], h->cnt);
-  if (G.ny > 1)
+  if ((rc = launch_check(h, "face_flux_x"))) return rc;
+  if (G.ny > 1) {
     k_face_flux<2, R, PT><<<nblocks((long long)G.nx * (G.ny + 1) * G.nz, 128), 128, 0, h->stream>>>(G, h->phys, P, (R *)h->F[1], h->cnt);
-  if (G.nz > 1)
+    if ((rc = launch_check(h, "face_flux_y"))) return rc;
+  }
+  if (G.nz > 1) {
     k_face_flux<3, R, PT><<<nblocks((long long)G.nx * G.ny * (G.nz + 1), 128), 128, 0, h->stream>>>(G, h->phys, P, (R *)h->F[2], h->cnt);
-  return launch_check(h);
+    if ((rc = launch_check(h, "face_flux_z"))) return rc;
+  }
+  return 0;
 }
 
 template <int MODE, class R, class PT>
@@ -103,7 +120,7 @@ int launch_update(grhd2_gpu *h, double dt) {
   k_cell_update<MODE, R, PT><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(
       G, h->phys, (PT *)h->P, (const R *)h->F[0], (const R *)h->F[1], (const R *)h->F[2], h->U, h->UP, h->RHS, dt,
       h->cfg.dx, h->cfg.dy, h->cfg.dz, h->cnt);
-  return launch_check(h);
+  return launch_check(h, MODE == 0 ? "cell_rhs" : "cell_update");
 }
 
 template <class R, class PT>
@@ -183,9 +200,9 @@ int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out) {
   if (c.precision_policy != GRHD2_PREC_FP64 && c.precision_policy != GRHD2_PREC_MIXED)
     return fail(h, GRHD2_ERR_ARG, "invalid precision policy %d", c.precision_policy);
   if (c.case_id == 12 && (c.nz % 2) != 0) return fail(h, GRHD2_ERR_BOUNDARY, "nz must be even for 3D trans-polar boundary conditions");
-  if ((c.case_id == 11 || c.case_id == 12) && c.ny > 1 && c.ny < c.nghost)
+  if ((c.case_id == 11 || c.case_id == 12) && c.ny < c.nghost)
     return fail(h, GRHD2_ERR_ARG, "reflecting/trans-polar boundaries need ny >= nghost");
-  if (c.case_id == 5 && (c.nx < c.nghost || (c.nz > 1 && c.nz < c.nghost)))
+  if (c.case_id == 5 && (c.nx < c.nghost || c.nz < c.nghost))
     return fail(h, GRHD2_ERR_ARG, "the jet's reflecting boundaries need nx, nz >= nghost");
   if (!(c.dx > 0) || (c.ny > 1 && !(c.dy > 0)) || (c.nz > 1 && !(c.dz > 0))) return fail(h, GRHD2_ERR_ARG, "grid spacing must be positive");
 
@@ -549,6 +566,40 @@ int grhd2_gpu_riemann_faces(grhd2_gpu *h, int n, int dir, const double *qL, cons
 int grhd2_gpu_physical_flux(grhd2_gpu *h, int n, int dir, const double *q, const double *alpha, const double *beta,
                             const double *gamma, const double *sqg, double *flux) {
   return faces_common(h, n, dir, q, nullptr, alpha, beta, gamma, sqg, flux, 1);
+}
+
+int grhd2_gpu_get_stream(grhd2_gpu *h, void **stream_out) {
+  if (!h || !stream_out) return GRHD2_ERR_ARG;
+  *stream_out = (void *)h->stream;
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_profile_step(grhd2_gpu *h, double dt, float *ms, const char **names, int cap, int *n_out) {
+  if (int rc = ready(h, true)) return rc;
+  cudaEvent_t start;
+  CUDA_TRY(h, cudaEventCreate(&start));
+  CUDA_TRY(h, cudaEventRecord(start, h->stream));
+  h->profiling = true;
+  int rc = step_dispatch(h, dt);
+  h->profiling = false;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  const int n = (int)h->prof_ev.size();
+  for (int k = 0; k < n; ++k) {
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, k == 0 ? start : h->prof_ev[k - 1], h->prof_ev[k]);
+    if (k < cap) {
+      if (ms) ms[k] = t;
+      if (names) names[k] = h->prof_names[k];
+    }
+  }
+  for (auto ev : h->prof_ev) cudaEventDestroy(ev);
+  cudaEventDestroy(start);
+  h->prof_ev.clear();
+  h->prof_names.clear();
+  if (n_out) *n_out = n;
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(h, GRHD2_ERR_CUDA, "profile step: %s", cudaGetErrorString(e));
+  return GRHD2_OK;
 }
 
 int grhd2_gpu_synchronize(grhd2_gpu *h) {

@@ -403,6 +403,9 @@ __global__ void k_prims_out(const GridDev G, const PT *__restrict__ Pin, double 
   const int j = (int)(r % NY) - G.ng, k = (int)(r / NY) - G.ng;
   const bool oi = i < 1 || i > G.nx, oj = j < 1 || j > G.ny, ok = k < 1 || k > G.nz;
   if ((int)oi + (int)oj + (int)ok > 1) return;
+  // index -nghost is never written by set_boundary_conditions (it keeps the caller's
+  // value), except in the jet case, which resets every ghost to the ambient state
+  if (G.case_id != 5 && (i == -G.ng || j == -G.ng || k == -G.ng)) return;
   double q[NEQ];
   if (oj) load_cell<2>(Pin, G, i, j, k, q);
   else if (ok) load_cell<3>(Pin, G, i, j, k, q);

@@ -55,6 +55,40 @@ template <class R> __device__ __forceinline__ R eps_of();
 template <> __device__ __forceinline__ double eps_of<double>() { return DBL_EPSILON; }
 template <> __device__ __forceinline__ float eps_of<float>() { return FLT_EPSILON; }
 
+// exp for the WENO3 adaptive epsilon (reconstruction.f90:169).  CUDA's exp and the host C
+// library's (which the reference calls) round differently in the last bit, and a one-ulp
+// difference flips downstream branches (MP5's "< 1e-10" test, the HLLC tolerances), so the
+// kernels and the CPU oracle evaluate exp with one published method and the same
+// operation order: Cody-Waite reduction x = k ln2 + r, k = rint(x/ln2), ln2 split into a
+// 32-bit head and a tail; e^r by its Taylor series through r^13/13! on |r| <= ln2/2
+// (truncation below 5e-18 relative) in Horner form; exact scaling by 2^k.  Accurate to
+// about one ulp.
+__device__ __forceinline__ double exp_cw(double x) {
+  if (x != x) return x;
+  if (x > 709.78) return HUGE_VAL;
+  if (x < -745.2) return 0.0;
+  const double log2e = 0x1.71547652b82fep+0;
+  const double ln2_hi = 0x1.62e42feep-1;        // ln 2 to 32 significant bits
+  const double ln2_lo = 0x1.a39ef35793c76p-33;  // ln 2 - ln2_hi
+  const double k = rint(x * log2e);
+  const double r = (x - k * ln2_hi) - k * ln2_lo;
+  double p = 1.0 / 6227020800.0;
+  p = 1.0 / 479001600.0 + r * p;
+  p = 1.0 / 39916800.0 + r * p;
+  p = 1.0 / 3628800.0 + r * p;
+  p = 1.0 / 362880.0 + r * p;
+  p = 1.0 / 40320.0 + r * p;
+  p = 1.0 / 5040.0 + r * p;
+  p = 1.0 / 720.0 + r * p;
+  p = 1.0 / 120.0 + r * p;
+  p = 1.0 / 24.0 + r * p;
+  p = 1.0 / 6.0 + r * p;
+  p = 0.5 + r * p;
+  p = 1.0 + r * p;
+  return ldexp(1.0 + r * p, (int)k);
+}
+__device__ __forceinline__ float exp_cw(float x) { return expf(x); }  // mixed policy: FP32
+
 // ------------------------------------------------------------------------------------
 // reconstruction.f90:28-278
 // ------------------------------------------------------------------------------------
@@ -77,7 +111,7 @@ template <class R> __device__ __forceinline__ R weno3(R qm, R q0, R qp) {
   R t0 = q0 - qp, t1 = qm - q0;
   R b0 = t0 * t0, b1 = t1 * t1;
   R sensor = fabs(b0 - b1) / (rmax(b0, b1) + eps_min);
-  R eh = eps_min + (qm * qm + q0 * q0 + qp * qp) * exp(R(-10) * sensor);
+  R eh = eps_min + (qm * qm + q0 * q0 + qp * qp) * exp_cw(R(-10) * sensor);
   R e0 = eh + b0, e1 = eh + b1;
   R a0 = d0 / (e0 * e0), a1 = d1 / (e1 * e1);
   R w0 = a0 / (a0 + a1), w1 = a1 / (a0 + a1);

@@ -90,6 +90,9 @@ GPU_SYMBOLS = {
     "grhd2_gpu_physical_flux": (C.c_int, [_VP, C.c_int, C.c_int, c_double_p, c_double_p,
                                           c_double_p, c_double_p, c_double_p, c_double_p]),
     "grhd2_gpu_synchronize": (C.c_int, [_VP]),
+    "grhd2_gpu_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "grhd2_gpu_profile_step": (C.c_int, [_VP, C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_char_p),
+                                         C.c_int, C.POINTER(C.c_int)]),
     "grhd2_gpu_last_error": (C.c_char_p, [_VP]),
     "grhd2_gpu_destroy": (None, [_VP]),
     "grhd2_gpu_abi_version": (C.c_int, []),

@@ -113,11 +113,13 @@ class GpuGrid:
         self._check(self.lib.grhd2_gpu_calc_rhs(self._h, N.dptr(rhs)))
         return rhs
 
-    def download(self, p_template: np.ndarray | None = None):
+    def download(self, p_template: np.ndarray | None = None, want_up: bool = True, want_p: bool = True):
         """(up, p): p holds interior cells and single-direction ghosts; the remaining
         ghost entries keep the values of p_template (zeros by default)."""
-        up = np.empty(self.problem.cons_shape)
-        p = np.zeros(self.problem.prim_shape) if p_template is None else np.array(p_template, dtype=np.float64)
+        up = np.empty(self.problem.cons_shape) if want_up else None
+        p = None
+        if want_p:
+            p = np.zeros(self.problem.prim_shape) if p_template is None else np.array(p_template, dtype=np.float64)
         self._check(self.lib.grhd2_gpu_download(self._h, N.dptr(up), N.dptr(p)))
         return up, p
 
@@ -131,6 +133,22 @@ class GpuGrid:
 
     def synchronize(self):
         self._check(self.lib.grhd2_gpu_synchronize(self._h))
+
+    @property
+    def stream_ptr(self) -> int:
+        """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        s = C.c_void_p()
+        self._check(self.lib.grhd2_gpu_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def profile_step(self, dt: float):
+        """[(kernel name, ms)] for every launch of one step."""
+        cap = 64
+        ms = (C.c_float * cap)()
+        names = (C.c_char_p * cap)()
+        n = C.c_int()
+        self._check(self.lib.grhd2_gpu_profile_step(self._h, dt, ms, names, cap, C.byref(n)))
+        return [(names[k].decode(), float(ms[k])) for k in range(min(n.value, cap))]
 
     # ---- single-face entry points ------------------------------------------------------
     def riemann_faces(self, dir: int, qL, qR, alpha, beta, gamma, sqg) -> np.ndarray:

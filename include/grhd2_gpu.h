@@ -148,6 +148,14 @@ int grhd2_gpu_physical_flux(grhd2_gpu *h, int n, int dir, const double *q, const
                             double *flux);
 /* Wait for all work of the handle; returns the first asynchronous error. */
 int grhd2_gpu_synchronize(grhd2_gpu *h);
+/* The handle's CUDA stream (a cudaStream_t) so callers can order their own work and
+ * record timing events on it.  No reference counterpart (the reference has no device). */
+int grhd2_gpu_get_stream(grhd2_gpu *h, void **stream_out);
+/* One SSP-RK3 step with a CUDA event around every kernel: ms[k] is the duration of the
+ * k-th launch, names[k] its kernel ("face_flux_x", "cell_update", ...); *n_out launches
+ * (at most cap are reported).  Observability for the per-stage timers the reference
+ * lacks (its only timer is omp_get_wtime around the whole run, grhd2.f90:303-330). */
+int grhd2_gpu_profile_step(grhd2_gpu *h, double dt, float *ms, const char **names, int cap, int *n_out);
 const char *grhd2_gpu_last_error(const grhd2_gpu *h);
 void grhd2_gpu_destroy(grhd2_gpu *h);
 int grhd2_gpu_abi_version(void);

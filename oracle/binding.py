@@ -14,6 +14,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "libgrhd2_oracle.so")
+# the same oracle calling the C library's exp (as the reference build does) in WENO3
+LIB_LIBM = os.path.join(HERE, "lib", "libgrhd2_oracle_libm.so")
 _dp = C.POINTER(C.c_double)
 
 
@@ -41,7 +43,7 @@ class OrcCounters(C.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
-_lib = None
+_libs = {}
 
 
 def build():
@@ -49,12 +51,12 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
+def lib(libm_exp: bool = False):
+    path = LIB_LIBM if libm_exp else LIB
+    if path not in _libs:
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(LIB)
+        L = C.CDLL(path)
         P, M, K = C.POINTER(OrcConfig), C.POINTER(OrcMetric), C.POINTER(OrcCounters)
         sig = {
             "orc_calc_rhs": (None, [P, M, _dp, _dp, K]),
@@ -70,12 +72,13 @@ def lib():
             "orc_step": (C.c_int, [P, M, _dp, _dp, _dp, _dp, C.c_double, K]),
             "orc_run": (C.c_int64, [P, M, _dp, _dp, C.c_double, C.c_double, C.c_int64, _dp, K]),
             "orc_num_threads": (C.c_int, []),
+            "orc_exp": (C.c_double, [C.c_double]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def _p(a):
@@ -116,7 +119,7 @@ def metric_from(mv, bv) -> OrcMetric:
 class OracleRun:
     """Oracle state for one problem: p (ghosted) and up (interior), reference layout."""
 
-    def __init__(self, problem, p=None):
+    def __init__(self, problem, p=None, libm_exp: bool = False):
         self.problem = problem
         self.cfg = config_from(problem.config(0))
         self._mv = problem.metric_view()
@@ -125,7 +128,7 @@ class OracleRun:
         self.p = (problem.initial_prims() if p is None else p.copy())
         self.up = np.zeros(problem.cons_shape)
         self.counters = OrcCounters()
-        self.L = lib()
+        self.L = lib(libm_exp)
 
     def prim_to_cons(self):
         self.L.orc_prim_to_cons_all(C.byref(self.cfg), C.byref(self.met), _p(self.p), _p(self.up))

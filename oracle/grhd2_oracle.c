@@ -48,6 +48,46 @@ static inline double max5(double a, double b, double c, double d, double e) {
 static inline double min5(double a, double b, double c, double d, double e) {
   return fmin_ref(min4(a, b, c, d), e);
 }
+/* exp(x) for the WENO3 adaptive epsilon (reconstruction.f90:169).  The reference calls
+ * the C library's exp, whose last-bit rounding the CUDA exp does not share; a one-ulp
+ * difference there flips downstream branches (MP5's "< 1e-10" test, HLLC tolerances) and
+ * breaks bit-level parity.  Both this oracle and the kernels therefore evaluate exp with
+ * the same published method: Cody-Waite reduction x = k ln2 + r, k = rint(x/ln2), ln2
+ * split into a 32-bit head and a tail; e^r by the Taylor series through r^13/13!
+ * (|r| <= ln2/2, truncation below 5e-18 relative) in Horner form; exact scaling by 2^k.
+ * It differs from a correctly rounded exp by at most about one ulp.  Build with
+ * -DORC_LIBM_EXP to use the C library's exp instead. */
+static double exp_cw(double x) {
+#ifdef ORC_LIBM_EXP
+  return exp(x);
+#else
+  if (x != x) return x;
+  if (x > 709.78) return HUGE_VAL;
+  if (x < -745.2) return 0.0;
+  const double log2e = 0x1.71547652b82fep+0;
+  const double ln2_hi = 0x1.62e42feep-1;         /* ln 2 to 32 significant bits */
+  const double ln2_lo = 0x1.a39ef35793c76p-33;   /* ln 2 - ln2_hi */
+  const double k = rint(x * log2e);
+  const double r = (x - k * ln2_hi) - k * ln2_lo;
+  double p = 1.0 / 6227020800.0;
+  p = 1.0 / 479001600.0 + r * p;
+  p = 1.0 / 39916800.0 + r * p;
+  p = 1.0 / 3628800.0 + r * p;
+  p = 1.0 / 362880.0 + r * p;
+  p = 1.0 / 40320.0 + r * p;
+  p = 1.0 / 5040.0 + r * p;
+  p = 1.0 / 720.0 + r * p;
+  p = 1.0 / 120.0 + r * p;
+  p = 1.0 / 24.0 + r * p;
+  p = 1.0 / 6.0 + r * p;
+  p = 0.5 + r * p;
+  p = 1.0 + r * p;
+  return ldexp(1.0 + r * p, (int)k);
+#endif
+}
+
+double orc_exp(double x) { return exp_cw(x); }
+
 /* Fortran sign(1.0d0, x): honours the sign bit, including -0.0 */
 static inline double sgn1(double x) { return copysign(1.0, x); }
 static inline int isfin(double x) { return isfinite(x); }
@@ -128,7 +168,7 @@ static double weno3_interface(const double *q) {
   double beta_0 = t0 * t0;
   double beta_1 = t1 * t1;
   double shock_sensor = fabs(beta_0 - beta_1) / (fmax_ref(beta_0, beta_1) + eps_min);
-  double eps_hybrid = eps_min + (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * exp(-10.0 * shock_sensor);
+  double eps_hybrid = eps_min + (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * exp_cw(-10.0 * shock_sensor);
   double e0 = eps_hybrid + beta_0, e1 = eps_hybrid + beta_1;
   double alpha_0 = d0 / (e0 * e0);
   double alpha_1 = d1 / (e1 * e1);

@@ -106,6 +106,8 @@ int64_t orc_run(const orc_config *c, const orc_metric *m, double *up, double *p,
                 orc_counters *cnt);
 /* number of OpenMP threads used by orc_run / orc_step (1 without OpenMP) */
 int orc_num_threads(void);
+/* the exp used by WENO3 (reconstruction.f90:169), exposed for its accuracy test */
+double orc_exp(double x);
 
 #ifdef __cplusplus
 }

@@ -12,7 +12,9 @@ pytestmark = pytest.mark.gpu
 
 
 def grid(metric_ks: bool, rs: str):
-    pb = torus_2p5d(nx=8, nz=4, rs=rs) if metric_ks else shock_tube(nx=8, rs=rs)
+    # Gamma = 4/3 as in the fixture of tests/test_hllc_fluxes.f90:11
+    pb = (torus_2p5d(nx=8, nz=4, rs=rs) if metric_ks
+          else shock_tube(nx=8, rs=rs, adiabatic_index=1.3333333333333333))
     return GpuGrid(pb, upload_initial=False)
 
 

@@ -292,3 +292,15 @@ def test_dust_boundaries():
     assert at(q, g, 0, 1, 1)[0] == at(q, g, 1, 1, 1)[0]
     assert np.array_equal(at(q, g, nx + 1, 1, 1), outer[0])
     assert np.array_equal(at(q, g, 2, 0, 1), at(q, g, 2, ny, 1))
+
+
+def test_weno3_exp_accuracy():
+    """The exp shared by the oracle and the kernels (Cody-Waite + Taylor) stays within
+    one ulp of the C library's exp over the WENO3 argument range and beyond."""
+    L = B.lib()
+    xs = np.concatenate([np.linspace(-10.0, 0.0, 20001), np.linspace(-700.0, 700.0, 20001),
+                         np.random.default_rng(3).uniform(-12, 1, 20000)])
+    for x in xs:
+        a, b = L.orc_exp(float(x)), float(np.exp(x))
+        assert abs(a - b) <= np.spacing(b), (x, a, b)
+    assert L.orc_exp(0.0) == 1.0
