@@ -3,13 +3,15 @@
 
 Workload (N=1): the 2.5D equatorial Fishbone-Moncrief torus in Kerr-Schild coordinates
 (a = 0.9), log-r spheroidal grid 400 x 1 x 200, WENO5 + HLLE, r_in 6, r_max 12, Gamma 4/3,
-1% seeded pressure noise -- synthetic initial data of the configuration's shape.  One
-"step" is one full SSP-RK3 step (3 RHS evaluations, stage combinations, con2prim sweeps
-and boundary fills) of the whole grid.  The headline value is the FP64 path (the parity
-path); the mixed FP32/FP64 policy is reported beside it with its L1 against FP64.
+1% seeded pressure noise -- synthetic initial data of the configuration's shape.  A batch
+of --batch such grids (default 32, one perturbation seed each) steps together: one launch
+per kernel kind for all of them, each step replayed as one CUDA graph.  One "step" is one
+full SSP-RK3 step (3 RHS evaluations, stage combinations, con2prim sweeps and boundary
+fills) of every grid of the batch.  The headline value is the FP64 path (the parity
+path); the mixed FP32/FP64 policy and a single grid alone are reported beside it.
 
-Multi-GPU: one process per GPU (torchrun), each rank advances its own replica of the
-workload ("replicas only": the reference path does not shard); the value is the
+Multi-GPU: one process per GPU (torchrun), each rank advances its own batch
+("replicas only": the grids are independent, nothing is exchanged); the value is the
 whole-job zone-updates/s, timed on the device as the max over ranks.
 
 ``--impl reference`` times the reference's CPU implementation of the path on the host
@@ -36,7 +38,7 @@ METRIC = "zone-updates/s per SSP-RK3 step, FP32-mixed vs FP64 at stated L1; serv
 WORKLOAD = "2.5D Kerr-Schild FM torus 400x1x200, WENO5+HLLE, a=0.9, r_in=6, r_max=12, Gamma=4/3"
 
 
-def torus_problem(nx=400, nz=200):
+def torus_problem(nx=400, nz=200, seed=3435):
     from grhd_b200.problem import Problem
     keys = dict(metric="kerr_schild", geometry="spheroidal", logarithmic_r=True, spin=0.9, bh_mass=1.0,
                 nx=nx, ny=1, nz=nz, r_min=1.2, r_max=40.0, theta_min=0, theta_max=1, phi_min=0,
@@ -44,7 +46,7 @@ def torus_problem(nx=400, nz=200):
                 fm_polytropic_constant=0.0015, adiabatic_index=1.3333333333333333,
                 reconstruction="weno5", riemann_solver="hlle", shock_sensor=False, cfl=0.4,
                 perturbation="pressure_noise", perturbation_amplitude=0.01, perturbation_time=0.0,
-                perturbation_seed=3435)
+                perturbation_seed=seed)
     return Problem.from_keys("fishbone_equatorial", **keys)
 
 
@@ -127,149 +129,209 @@ def measured_peaks():
 
 
 def kernel_bytes(name: str, pb, mixed: bool) -> float:
-    """Algorithmic DRAM bytes of one launch: every cell's state read or written once,
-    every face flux written once by face_flux and read once by cell_update.  Metric
-    tables (k-invariant, L2-resident) and stencil re-reads are excluded."""
+    """Algorithmic DRAM bytes of one launch for one grid: each array the kernel must touch,
+    read or written once.  Metric tables (k-invariant, L2-resident) and stencil re-reads
+    are excluded.  recon_d reads P and writes q_L, q_R; riemann_d reads q_L, q_R and writes
+    the face fluxes; cell_update reads the fluxes, P, up and u (or writes u in stage 1) and
+    writes P and up."""
     nx, ny, nz = pb.nx, pb.ny, pb.nz
     n = nx * ny * nz
-    ep = 4 if mixed else 8   # primitive / flux element size
+    ep = 4 if mixed else 8   # primitive / interface / flux element size
     nf = {"x": (nx + 1) * ny * nz, "y": nx * (ny + 1) * nz, "z": nx * ny * (nz + 1)}
-    if name.startswith("face_flux_"):
-        return 5 * ep * n + 5 * ep * nf[name[-1]]
+    if name.startswith("recon_"):
+        return 5 * ep * n + 10 * ep * nf[name[-1]]
+    if name.startswith("riemann_"):
+        return 15 * ep * nf[name[-1]]
     if name == "cell_update":
         flux_read = 5 * ep * (nf["x"] + (nf["y"] if ny > 1 else 0) + (nf["z"] if nz > 1 else 0))
-        # P read+write, up read+write, u read (stages 2,3) or write (stage 1)
-        return 2 * 5 * ep * n + 3 * 5 * 8 * n + flux_read
+        return flux_read + 2 * 5 * ep * n + 3 * 5 * 8 * n
     return 0.0
 
 
+STEP_BYTES_PER_ZONE = {"fp64": 600.0, "mixed": 600.0}
+"""Algorithmic bytes of one zone-update (a cell through a full SSP-RK3 step): per stage
+read P, u, up, write up, P (5 values each); the mixed policy stores P in FP32 but keeps a
+separate FP64 state, so the same 600 B are counted for both."""
+
+
 # ------------------------------------------------------------------------------------
+def make_batch(nbatch, precision, stream, seed0=3435):
+    """nbatch torus grids (perturbation seeds seed0, seed0+1, ...) on one stream, each
+    running on its own device clock with its CFL dt."""
+    from grhd_b200.solver import GpuBatch, GpuGrid
+    grids = []
+    for r in range(nbatch):
+        pb = torus_problem(seed=seed0 + r)
+        g = GpuGrid(pb, precision=precision, upload_initial=False, stream=stream.cuda_stream)
+        g.upload(p=initial_state(pb))
+        g.prim_to_cons()
+        grids.append(g)
+    b = GpuBatch(grids)
+    for k in range(nbatch):
+        b.set_clock(k, 0.0, 1e300, -1)
+    return grids, b
+
+
+def close_batch(grids, b):
+    b.close()
+    for g in grids:
+        g.close()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from grhd_b200.solver import GpuGrid
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     pb = torus_problem()
-    p0 = initial_state(pb)
     ncell = pb.n_cells
+    stream = torch.cuda.Stream()
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def timed_run(precision):
-        g = GpuGrid(pb, precision=precision, upload_initial=False)
-        g.upload(p=p0)
-        g.prim_to_cons()
-        dt = g.cfl()
-        ext = torch.cuda.ExternalStream(g.stream_ptr)
-        for _ in range(args.warmup):
-            g.step(dt)
-        g.synchronize()
+    def max_over_ranks(ms):
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    def timed(b, flush):
+        """ms of args.steps batched steps (graph replays), CUDA events on the batch's stream."""
+        b.step(args.warmup, graph=True)
+        torch.cuda.synchronize()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
         for s in range(args.steps):
-            with torch.cuda.stream(ext):
-                l2_flush.zero_()  # evict the ~20 MB working set from the 126 MB L2
-            evs[s][0].record(ext)
-            g.step(dt)
-            evs[s][1].record(ext)
-        g.synchronize()
+            if flush:
+                with torch.cuda.stream(stream):
+                    l2_flush.zero_()
+            evs[s][0].record(stream)
+            b.step(1, graph=True)
+            evs[s][1].record(stream)
         torch.cuda.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in evs)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return g, dt, ms
+        return max_over_ranks(sum(a.elapsed_time(c) for a, c in evs))
 
+    nb = args.batch
     with ClockSampler(local) as clk:
-        g64, dt, ms64 = timed_run("fp64")
+        g64, b64 = make_batch(nb, "fp64", stream)
+        ms64 = timed(b64, flush=False)
     clocks = clk.summary()
-    gmx, _, msmx = timed_run("mixed")
+    gmx, bmx = make_batch(nb, "mixed", stream)
+    msmx = timed(bmx, flush=False)
     # L1 of the mixed policy against FP64 after the same steps from the same state
-    up64, _ = g64.download()
-    upmx, _ = gmx.download()
+    up64 = g64[0].download(want_p=False)[0]
+    upmx = gmx[0].download(want_p=False)[0]
     den = np.abs(up64.reshape(-1, 5)).sum(axis=0)
-    l1_mixed = (np.abs(upmx - up64).reshape(-1, 5).sum(axis=0) / den).tolist()
+    num = np.abs(upmx - up64).reshape(-1, 5).sum(axis=0)
+    # a variable that is zero everywhere (S_y of the equatorial torus) reports its absolute L1
+    l1_mixed = np.where(den > 0, num / np.where(den > 0, den, 1.0), num).tolist()
+    n_done = b64.clock(0)[1]
+    close_batch(gmx, bmx)
 
-    # per-kernel durations of one step (outside the timed region) -> dominant kernel
+    # one grid alone (L2 flushed between steps: its ~22 MB working set fits in L2)
+    singles = {}
+    for prec in ("fp64", "mixed"):
+        gs, bs = make_batch(1, prec, stream)
+        ms = timed(bs, flush=True)
+        singles[prec] = {"value": world * ncell * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps}
+        close_batch(gs, bs)
+
+    # per-kernel durations of one batched step (outside the timed region) -> dominant kernel
     prof = {}
-    for _ in range(3):
-        for name, t in g64.profile_step(dt):
+    reps = 3
+    for _ in range(reps):
+        for name, t in b64.profile_step():
             prof.setdefault(name, []).append(t)
-    per_step = {k: sum(v) / 3.0 for k, v in prof.items()}
-    launches = {k: len(v) // 3 for k, v in prof.items()}
+    per_step = {k: sum(v) / reps for k, v in prof.items()}
+    launches = {k: len(v) // reps for k, v in prof.items()}
     dom = max(per_step, key=per_step.get)
     dom_ms = per_step[dom] / launches[dom]
-    dom_bytes = kernel_bytes(dom, pb, False)
+    dom_bytes = kernel_bytes(dom, pb, False) * nb
     peak, peak_kind = measured_peaks()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tr_path):
         with open(tr_path) as f:
-            traffic = json.load(f).get(dom)
+            tr = json.load(f).get("torus2p5d_400x1x200", {}).get(dom)
+        traffic = tr * nb if tr is not None else None
 
-    # end to end through the C-ABI with host buffers (pinned), copies inside the timed region
-    pin_p = torch.from_numpy(p0.copy()).pin_memory()
-    pin_up = torch.empty(pb.cons_shape, dtype=torch.float64).pin_memory()
-    g_e = GpuGrid(pb, precision="fp64", upload_initial=False)
-    g_e.upload(p=p0)
-    g_e.prim_to_cons()
-    up_e, _ = g_e.download()
-    pin_up.numpy()[...] = up_e
-    ext = torch.cuda.ExternalStream(g_e.stream_ptr)
-    h2d = pin_up.numel() * 8 + pin_p.numel() * 8
-    lib, h = g_e.lib, g_e._h
+    # end to end through the C-ABI with host buffers (pinned): every step uploads each grid's
+    # conserved state, recovers primitives, steps the batch, downloads the conserved state
     from grhd_b200 import native as N
-    pu, pp = N.dptr(pin_up.numpy()), N.dptr(pin_p.numpy())
-    for _ in range(args.warmup):
-        lib.grhd2_gpu_upload(h, pu, pp)
-        lib.grhd2_gpu_step(h, dt)
-        lib.grhd2_gpu_download(h, pu, pp)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    for _ in range(args.steps):
-        assert lib.grhd2_gpu_upload(h, pu, pp) == 0
-        assert lib.grhd2_gpu_step(h, dt) == 0
-        assert lib.grhd2_gpu_download(h, pu, pp) == 0
-    e1.record(ext)
-    torch.cuda.synchronize()
-    ms_e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e = float(t.item())
+    lib = g64[0].lib
+    pins = []
+    for g in g64:
+        up = torch.empty(pb.cons_shape, dtype=torch.float64).pin_memory()
+        up.numpy()[...] = g.download(want_p=False)[0]
+        pins.append(up)
+    ptrs = [N.dptr(u.numpy()) for u in pins]
+    h2d = sum(u.numel() * 8 for u in pins)
 
-    value = world * ncell * args.steps / (ms64 * 1e-3)
+    def e2e_step():
+        for g, pu in zip(g64, ptrs):
+            assert lib.grhd2_gpu_upload(g._h, pu, None) == 0
+            assert lib.grhd2_gpu_cons_to_prim_all(g._h) == 0
+        b64.step(1, graph=True)
+        for g, pu in zip(g64, ptrs):
+            assert lib.grhd2_gpu_download(g._h, pu, None) == 0
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e = max_over_ranks(e0.elapsed_time(e1))
+    close_batch(g64, b64)
+
+    value = world * nb * ncell * args.steps / (ms64 * 1e-3)
+    mixed_value = world * nb * ncell * args.steps / (msmx * 1e-3)
     out = {
         "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms64 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (analytic torus initial data, seeded pressure noise)",
-        "config": {"workload": WORKLOAD, "nx": pb.nx, "ny": pb.ny, "nz": pb.nz, "cells": ncell,
-                   "precision": "fp64 (parity path, no FMA)", "parallelism": f"replicas x{world}",
-                   "l2": "256 MB buffer written between timed steps (working set ~20 MB < L2)"},
-        "variants": {"mixed": {"value": world * ncell * args.steps / (msmx * 1e-3),
-                               "ms_per_step": msmx / args.steps, "dtype": "f32 recon/Riemann/sources, f64 con2prim + RK",
-                               "l1_vs_fp64": l1_mixed}},
+        "data": "synthetic (analytic torus initial data, seeded pressure noise, one seed per grid)",
+        "config": {"workload": WORKLOAD, "grids_per_gpu": nb, "nx": pb.nx, "ny": pb.ny, "nz": pb.nz,
+                   "cells_per_gpu": nb * ncell, "precision": "fp64 (parity path, no FMA)",
+                   "parallelism": f"replicas x{world}", "graph": "one CUDA graph per batched step",
+                   "l2": f"inputs larger than L2: {nb} grids x ~22 MB resident state, no flush"},
+        "variants": {
+            "mixed_batched": {"value": mixed_value, "ms_per_step": msmx / args.steps,
+                              "dtype": "f32 recon/Riemann/sources, f64 con2prim + RK",
+                              "l1_vs_fp64": l1_mixed, "steps_compared": n_done,
+                              "speedup_vs_fp64_batched": mixed_value / value,
+                              "speedup_vs_fp64_single": mixed_value / singles["fp64"]["value"]},
+            "fp64_single_grid": dict(singles["fp64"], l2="256 MB buffer written between timed steps"),
+            "mixed_single_grid": dict(singles["mixed"], l2="256 MB buffer written between timed steps"),
+        },
         "clocks": clocks,
-        "e2e": {"value": world * ncell * args.steps / (ms_e * 1e-3), "unit": "zone-updates/s",
+        "e2e": {"value": world * nb * ncell * args.steps / (ms_e * 1e-3), "unit": "zone-updates/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
-                "path": "grhd2_gpu_upload(up,p) + grhd2_gpu_step + grhd2_gpu_download(up,p), pinned host buffers"},
+                "path": "per grid grhd2_gpu_upload(up) + grhd2_gpu_cons_to_prim_all, grhd2_gpu_batch_step, "
+                        "per grid grhd2_gpu_download(up); pinned host buffers"},
         "gpu_launches": sum(launches.values()) * args.steps,
         "kernels_ms_per_step": per_step,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms},
+                     "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
+                     "step": {"bytes_per_zone_update": STEP_BYTES_PER_ZONE["fp64"],
+                              "achieved": STEP_BYTES_PER_ZONE["fp64"] * value / world / 1e9,
+                              "frac": STEP_BYTES_PER_ZONE["fp64"] * value / world / 1e9 / peak,
+                              "mixed_achieved": STEP_BYTES_PER_ZONE["mixed"] * mixed_value / world / 1e9}},
     }
     if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(pb, p0, max_seconds=args.cpu_seconds)
+        out["cpu_baseline"] = cpu_baseline(pb, initial_state(pb), max_seconds=args.cpu_seconds)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -322,6 +384,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--batch", type=int, default=32, help="torus grids per GPU stepped as one batch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -63,18 +63,31 @@ def build_host(force=False, verbose=False) -> str:
 
 
 def build_gpu(force=False, verbose=False) -> str:
+    """Each .cu compiles to its own object in parallel, then one shared library links them.
+    --fmad=false keeps every multiply and add separately rounded (the FP64 parity path
+    must follow the reference's operation order)."""
     os.makedirs(LIB, exist_ok=True)
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
     out = os.path.join(LIB, "libgrhd2gpu.so")
     srcs = _sources("gpu", (".cu",))
-    deps = srcs + _sources("gpu", (".cuh", ".h")) + [os.path.join(INCLUDE, "grhd2_gpu.h")]
+    headers = _sources("gpu", (".cuh", ".h")) + [os.path.join(INCLUDE, "grhd2_gpu.h")]
     if not srcs:
         raise RuntimeError("no CUDA sources under grhd_b200/csrc/gpu")
-    if force or _newer(out, deps):
-        cmd = [_nvcc()] + ARCH + [
-            "-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
-            "-shared", "-I" + INCLUDE, "-I" + os.path.join(CSRC, "gpu"),
-            "-ccbin", _cxx(), "-o", out] + srcs
-        _run(cmd, verbose)
+    common = [_nvcc()] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
+                                 "-I" + INCLUDE, "-I" + os.path.join(CSRC, "gpu"), "-ccbin", _cxx()]
+    objs, jobs = [], []
+    for s in srcs:
+        o = os.path.join(obj_dir, os.path.splitext(os.path.basename(s))[0] + ".o")
+        objs.append(o)
+        if force or _newer(o, [s] + headers):
+            jobs.append(common + ["-c", "-o", o, s])
+    if jobs:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
+            list(ex.map(lambda c: _run(c, verbose), jobs))
+    if force or jobs or _newer(out, objs):
+        _run([_nvcc()] + ARCH + ["-shared", "-ccbin", _cxx(), "-o", out] + objs, verbose)
     return out
 
 

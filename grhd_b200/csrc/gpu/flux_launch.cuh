@@ -1,0 +1,46 @@
+// flux_launch.cuh -- host launchers of the face-flux kernels (compile-time dispatch on the
+// reconstruction scheme and the Riemann solver).  Included by one translation unit per
+// precision and kernel kind (recon_fp64.cu, riemann_fp64.cu, ...) so they compile in
+// parallel.  Every launch is batched: `map` lists, per block, the grid and its first face.
+#pragma once
+
+#include "flux.cuh"
+
+namespace grhd {
+
+template <int DIR, class R, class PT>
+inline void recon_dir(int rec, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
+  const dim3 grid((unsigned)nblocks, 5);
+  switch (rec) {
+    case REC_GODUNOV: k_recon<DIR, REC_GODUNOV, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
+    case REC_TVD: k_recon<DIR, REC_TVD, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
+    case REC_WENO3: k_recon<DIR, REC_WENO3, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
+    case REC_MP5: k_recon<DIR, REC_MP5, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
+    default: k_recon<DIR, REC_WENO5, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
+  }
+}
+
+template <class R, class PT>
+void launch_recon(int dir, int rec, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
+  if (nblocks <= 0) return;
+  if (dir == 1) recon_dir<1, R, PT>(rec, grids, map, nblocks, s);
+  else if (dir == 2) recon_dir<2, R, PT>(rec, grids, map, nblocks, s);
+  else recon_dir<3, R, PT>(rec, grids, map, nblocks, s);
+}
+
+template <class R>
+void launch_riemann(int dir, int rs, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
+  if (nblocks <= 0) return;
+  const unsigned nb = (unsigned)nblocks;
+  if (rs == RS_HLLC) {
+    if (dir == 1) k_riemann<1, RS_HLLC, R><<<nb, 128, 0, s>>>(grids, map);
+    else if (dir == 2) k_riemann<2, RS_HLLC, R><<<nb, 128, 0, s>>>(grids, map);
+    else k_riemann<3, RS_HLLC, R><<<nb, 128, 0, s>>>(grids, map);
+  } else {
+    if (dir == 1) k_riemann<1, RS_HLLE, R><<<nb, 128, 0, s>>>(grids, map);
+    else if (dir == 2) k_riemann<2, RS_HLLE, R><<<nb, 128, 0, s>>>(grids, map);
+    else k_riemann<3, RS_HLLE, R><<<nb, 128, 0, s>>>(grids, map);
+  }
+}
+
+}  // namespace grhd

@@ -1,15 +1,23 @@
 // grhd2_gpu.cu -- C-ABI of the B200 per-stage path (include/grhd2_gpu.h).
 //
-// One handle = one grid on the current device, one CUDA stream.  Device state:
+// One handle = one grid on one device and CUDA stream.  Device state of a grid:
 //   P      primitives, SoA interior planes (double, or float under the mixed policy)
 //   U, UP  conserved u and up of grhd2.f90:232-249, SoA interior planes (double)
-//   F[d]   face fluxes of direction d (double, or float under the mixed policy)
-//   tables k-invariant metric tables per (i,j) and per face (see state.cuh)
-// A step is 3 x (face_flux per active direction, cell_update); the first stage also
-// performs u = up.  Ghost cells are evaluated on load (state.cuh), so no boundary pass
-// runs between stages.
+//   Q      interface states q_L, q_R of the direction being processed
+//   F[d]   face fluxes of direction d
+//   tables k-invariant metric tables per (i,j) and per face (state.cuh)
+//   clock  t, final time, CFL dt, step count (state.cuh GridClock)
+// A step is, three times: for each active direction recon + riemann, then cell_update
+// (RHS, RK stage, con2prim; stage 1 also performs u = up); then the clocks advance.
+// Ghost cells are evaluated on load (state.cuh), so no boundary pass runs.
+//
+// Every stage launch is batched: a device array of grid descriptors plus a block map
+// (grid, first item) per kernel kind.  A handle steps as a batch of one; a
+// grhd2_gpu_batch steps many grids with one launch per kernel kind and scheme group, and
+// can replay the whole step as one CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -19,55 +27,115 @@
 #include <vector>
 
 #include "grhd2_gpu.h"
+#include "flux_launch.h"
 #include "frame.h"
 #include "kernels.cuh"
 
 using namespace grhd;
 
+namespace {
+
+int vfail(std::string &err, int code, const char *fmt, va_list ap) {
+  char buf[512];
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  err = buf;
+  return code;
+}
+
+// kernel kinds of a step and their items-per-block
+enum Kind { K_RECON_X = 0, K_RIEMANN_X, K_RECON_Y, K_RIEMANN_Y, K_RECON_Z, K_RIEMANN_Z, K_CELL, NKIND };
+const int KIND_BS[NKIND] = {RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, CELL_BS};
+const char *KIND_NAME[NKIND] = {"recon_x", "riemann_x", "recon_y", "riemann_y", "recon_z", "riemann_z", "cell_update"};
+
+long long kind_items(const GridDev &G, int k) {
+  if (k == K_CELL) return G.ncell;
+  const int dir = k / 2 + 1;
+  if (dir == 2 && G.ny == 1) return 0;
+  if (dir == 3 && G.nz == 1) return 0;
+  if (dir == 1) return (long long)(G.nx + 1) * G.ny * G.nz;
+  if (dir == 2) return (long long)G.nx * (G.ny + 1) * G.nz;
+  return (long long)G.nx * G.ny * (G.nz + 1);
+}
+
+inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+bool bit_equal(double a, double b) { return std::memcmp(&a, &b, sizeof a) == 0; }
+
+}  // namespace
+
+struct grhd2_gpu_batch;
+
 struct grhd2_gpu {
   grhd2_gpu_config cfg{};
-  Phys phys{};
-  GridDev G{};
+  GridDev G{};  // host copy of the device descriptor (device pointers inside)
   int device = 0;
-  bool mixed = false;
+  bool mixed = false, own_stream = false;
   cudaStream_t stream = nullptr;
-  // device buffers
-  void *P = nullptr;
-  double *U = nullptr, *UP = nullptr, *RHS = nullptr;
-  void *F[3] = {nullptr, nullptr, nullptr};
+  // owned device buffers (their addresses are also in G)
   double *centre = nullptr, *face[3] = {nullptr, nullptr, nullptr};
   double *inj = nullptr, *dust = nullptr, *xc = nullptr, *frozen[3] = {nullptr, nullptr, nullptr};
-  unsigned long long *cnt = nullptr, *red = nullptr;
+  unsigned long long *red = nullptr;
   double *staging = nullptr;
   size_t n_ghosted = 0, n_interior = 0;
+  GridClock hclock{};  // host mirror of the device clock
+  int version = 0;     // bumped whenever G changes (batches refresh their device copies)
   bool metric_set = false, bc_set = false, prims_set = false, cons_set = false;
   double dt_cache = 0.0;
   bool dt_valid = false;
+  grhd2_gpu_batch *self = nullptr;  // batch of one used by step/run/calc_rhs
   std::string err;
-  // per-launch timing (grhd2_gpu_profile_step): events recorded after every launch
+};
+
+struct Group {
+  bool mixed;
+  int rec, rs;
+  std::vector<int> members;
+  BlockMap *d_map = nullptr;
+  int off[NKIND], nb[NKIND];
+};
+
+struct grhd2_gpu_batch {
+  std::vector<grhd2_gpu *> m;
+  std::vector<int> versions;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  GridDev *d_grids = nullptr;
+  std::vector<Group> groups;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;
   std::vector<const char *> prof_names;
-  bool profiling = false;
+  std::string err;
 };
 
 namespace {
 
 int fail(grhd2_gpu *h, int code, const char *fmt, ...) {
-  if (h) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    h->err = buf;
-  }
+  if (!h) return code;
+  va_list ap;
+  va_start(ap, fmt);
+  vfail(h->err, code, fmt, ap);
+  va_end(ap);
+  return code;
+}
+int bfail(grhd2_gpu_batch *b, int code, const char *fmt, ...) {
+  if (!b) return code;
+  va_list ap;
+  va_start(ap, fmt);
+  vfail(b->err, code, fmt, ap);
+  va_end(ap);
   return code;
 }
 
-#define CUDA_TRY(h, call)                                                                        \
-  do {                                                                                           \
-    cudaError_t e_ = (call);                                                                     \
+#define CUDA_TRY(h, call)                                                                             \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
     if (e_ != cudaSuccess) return fail((h), GRHD2_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+#define BCUDA_TRY(b, call)                                                                             \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess) return bfail((b), GRHD2_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
 template <class T>
@@ -78,64 +146,143 @@ int dalloc(grhd2_gpu *h, T **p, size_t n) {
   return 0;
 }
 
-inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
-
-bool bit_equal(double a, double b) { return std::memcmp(&a, &b, sizeof a) == 0; }
-
-int launch_check(grhd2_gpu *h, const char *name = nullptr) {
+int launch_check(grhd2_gpu *h) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(h, GRHD2_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
-  if (h->profiling && name) {
+  return 0;
+}
+int blaunch_check(grhd2_gpu_batch *b, const char *name) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "kernel launch (%s): %s", name, cudaGetErrorString(e));
+  if (b->profiling) {
     cudaEvent_t ev;
-    if (cudaEventCreate(&ev) != cudaSuccess) return fail(h, GRHD2_ERR_CUDA, "cudaEventCreate failed");
-    cudaEventRecord(ev, h->stream);
-    h->prof_ev.push_back(ev);
-    h->prof_names.push_back(name);
+    if (cudaEventCreate(&ev) != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "cudaEventCreate failed");
+    cudaEventRecord(ev, b->stream);
+    b->prof_ev.push_back(ev);
+    b->prof_names.push_back(name);
   }
   return 0;
 }
 
-// ---- kernel dispatch ---------------------------------------------------------------
-template <class R, class PT>
-int launch_fluxes(grhd2_gpu *h) {
-  const GridDev &G = h->G;
-  const PT *P = (const PT *)h->P;
-  int rc;
-  k_face_flux<1, R, PT><<<nblocks(G.nface[0] * G.nz, 128), 128, 0, h->stream>>>(G, h->phys, P, (R *)h->F[0], h->cnt);
-  if ((rc = launch_check(h, "face_flux_x"))) return rc;
-  if (G.ny > 1) {
-    k_face_flux<2, R, PT><<<nblocks((long long)G.nx * (G.ny + 1) * G.nz, 128), 128, 0, h->stream>>>(G, h->phys, P, (R *)h->F[1], h->cnt);
-    if ((rc = launch_check(h, "face_flux_y"))) return rc;
+void destroy_batch_resources(grhd2_gpu_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  for (auto &g : b->groups) if (g.d_map) cudaFree(g.d_map);
+  b->groups.clear();
+  if (b->d_grids) cudaFree(b->d_grids);
+  b->d_grids = nullptr;
+}
+
+// (re)build device descriptors and block maps of a batch
+int build_batch(grhd2_gpu_batch *b) {
+  destroy_batch_resources(b);
+  const int n = (int)b->m.size();
+  std::vector<GridDev> hg(n);
+  b->versions.resize(n);
+  for (int g = 0; g < n; ++g) { hg[g] = b->m[g]->G; b->versions[g] = b->m[g]->version; }
+  BCUDA_TRY(b, cudaMalloc((void **)&b->d_grids, sizeof(GridDev) * n));
+  BCUDA_TRY(b, cudaMemcpyAsync(b->d_grids, hg.data(), sizeof(GridDev) * n, cudaMemcpyHostToDevice, b->stream));
+  for (int g = 0; g < n; ++g) {
+    const grhd2_gpu *h = b->m[g];
+    Group *grp = nullptr;
+    for (auto &x : b->groups)
+      if (x.mixed == h->mixed && x.rec == h->cfg.rec_method && x.rs == h->cfg.riemann) grp = &x;
+    if (!grp) {
+      b->groups.push_back(Group{h->mixed, h->cfg.rec_method, h->cfg.riemann, {}, nullptr, {}, {}});
+      grp = &b->groups.back();
+    }
+    grp->members.push_back(g);
   }
-  if (G.nz > 1) {
-    k_face_flux<3, R, PT><<<nblocks((long long)G.nx * G.ny * (G.nz + 1), 128), 128, 0, h->stream>>>(G, h->phys, P, (R *)h->F[2], h->cnt);
-    if ((rc = launch_check(h, "face_flux_z"))) return rc;
+  for (auto &grp : b->groups) {
+    std::vector<BlockMap> map;
+    for (int k = 0; k < NKIND; ++k) {
+      grp.off[k] = (int)map.size();
+      for (int g : grp.members) {
+        const long long items = kind_items(hg[g], k);
+        for (long long first = 0; first < items; first += KIND_BS[k]) map.push_back(BlockMap{g, (int)first});
+      }
+      grp.nb[k] = (int)map.size() - grp.off[k];
+    }
+    BCUDA_TRY(b, cudaMalloc((void **)&grp.d_map, sizeof(BlockMap) * std::max<size_t>(1, map.size())));
+    BCUDA_TRY(b, cudaMemcpyAsync(grp.d_map, map.data(), sizeof(BlockMap) * map.size(), cudaMemcpyHostToDevice, b->stream));
+  }
+  BCUDA_TRY(b, cudaStreamSynchronize(b->stream));  // host vectors go out of scope
+  return 0;
+}
+
+int refresh_batch(grhd2_gpu_batch *b) {
+  for (size_t g = 0; g < b->m.size(); ++g)
+    if (b->versions[g] != b->m[g]->version) return build_batch(b);
+  return 0;
+}
+
+// kind 0..5 for directions, then the cell kernel in MODE (0 rhs, 1..3 stages)
+template <class R, class PT>
+int enqueue_fluxes(grhd2_gpu_batch *b, const Group &grp) {
+  for (int d = 1; d <= 3; ++d) {
+    const int kr = 2 * (d - 1), ks = kr + 1;
+    if (grp.nb[kr] > 0) {
+      launch_recon<R, PT>(d, grp.rec, b->d_grids, grp.d_map + grp.off[kr], grp.nb[kr], b->stream);
+      if (int rc = blaunch_check(b, KIND_NAME[kr])) return rc;
+    }
+    if (grp.nb[ks] > 0) {
+      launch_riemann<R>(d, grp.rs, b->d_grids, grp.d_map + grp.off[ks], grp.nb[ks], b->stream);
+      if (int rc = blaunch_check(b, KIND_NAME[ks])) return rc;
+    }
   }
   return 0;
 }
 
 template <int MODE, class R, class PT>
-int launch_update(grhd2_gpu *h, double dt) {
-  const GridDev &G = h->G;
-  k_cell_update<MODE, R, PT><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(
-      G, h->phys, (PT *)h->P, (const R *)h->F[0], (const R *)h->F[1], (const R *)h->F[2], h->U, h->UP, h->RHS, dt,
-      h->cfg.dx, h->cfg.dy, h->cfg.dz, h->cnt);
-  return launch_check(h, MODE == 0 ? "cell_rhs" : "cell_update");
+int enqueue_cells(grhd2_gpu_batch *b, const Group &grp) {
+  if (grp.nb[K_CELL] <= 0) return 0;
+  k_cell_update<MODE, R, PT><<<grp.nb[K_CELL], CELL_BS, 0, b->stream>>>(b->d_grids, grp.d_map + grp.off[K_CELL]);
+  return blaunch_check(b, MODE == 0 ? "cell_rhs" : "cell_update");
 }
 
-template <class R, class PT>
-int do_step(grhd2_gpu *h, double dt) {
+template <int MODE>
+int enqueue_stage(grhd2_gpu_batch *b) {
+  for (const auto &grp : b->groups) {
+    int rc = grp.mixed ? enqueue_fluxes<float, float>(b, grp) : enqueue_fluxes<double, double>(b, grp);
+    if (rc) return rc;
+    rc = grp.mixed ? enqueue_cells<MODE, float, float>(b, grp) : enqueue_cells<MODE, double, double>(b, grp);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int enqueue_step(grhd2_gpu_batch *b) {
   int rc;
-  if ((rc = launch_fluxes<R, PT>(h))) return rc;
-  if ((rc = launch_update<1, R, PT>(h, dt))) return rc;
-  if ((rc = launch_fluxes<R, PT>(h))) return rc;
-  if ((rc = launch_update<2, R, PT>(h, dt))) return rc;
-  if ((rc = launch_fluxes<R, PT>(h))) return rc;
-  return launch_update<3, R, PT>(h, dt);
+  if ((rc = enqueue_stage<1>(b))) return rc;
+  if ((rc = enqueue_stage<2>(b))) return rc;
+  if ((rc = enqueue_stage<3>(b))) return rc;
+  const int n = (int)b->m.size();
+  k_advance_clocks<<<nblocks(n, 128), 128, 0, b->stream>>>(b->d_grids, n);
+  return blaunch_check(b, "advance_clocks");
 }
 
-int step_dispatch(grhd2_gpu *h, double dt) {
-  return h->mixed ? do_step<float, float>(h, dt) : do_step<double, double>(h, dt);
+int batch_steps(grhd2_gpu_batch *b, long long nsteps, bool use_graph) {
+  if (int rc = refresh_batch(b)) return rc;
+  if (nsteps <= 0) return 0;
+  if (!use_graph) {
+    for (long long s = 0; s < nsteps; ++s)
+      if (int rc = enqueue_step(b)) return rc;
+    return 0;
+  }
+  if (!b->exec) {
+    BCUDA_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(b);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    b->graph = g;
+    BCUDA_TRY(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+  }
+  for (long long s = 0; s < nsteps; ++s) BCUDA_TRY(b, cudaGraphLaunch(b->exec, b->stream));
+  return 0;
 }
 
 int ready(grhd2_gpu *h, bool need_state) {
@@ -146,6 +293,26 @@ int ready(grhd2_gpu *h, bool need_state) {
     return fail(h, GRHD2_ERR_STATE, "boundary data not set for case %d (call grhd2_gpu_set_bc_data)", cs);
   if (need_state && !(h->prims_set && h->cons_set)) return fail(h, GRHD2_ERR_STATE, "state not uploaded");
   CUDA_TRY(h, cudaSetDevice(h->device));
+  return 0;
+}
+
+int self_batch(grhd2_gpu *h) {
+  if (h->self) {
+    if (int rc = refresh_batch(h->self)) return fail(h, rc, "%s", h->self->err.c_str());
+    return 0;
+  }
+  grhd2_gpu_batch *b = new (std::nothrow) grhd2_gpu_batch();
+  if (!b) return fail(h, GRHD2_ERR_NOMEM, "out of host memory");
+  b->m.push_back(h);
+  b->device = h->device;
+  b->stream = h->stream;
+  h->self = b;
+  if (int rc = build_batch(b)) return fail(h, rc, "%s", b->err.c_str());
+  return 0;
+}
+
+int write_clock(grhd2_gpu *h) {
+  CUDA_TRY(h, cudaMemcpyAsync(h->G.clock, &h->hclock, sizeof(GridClock), cudaMemcpyHostToDevice, h->stream));
   return 0;
 }
 
@@ -174,6 +341,34 @@ int build_face_table(grhd2_gpu *h, std::vector<double> &T, size_t n, int dir, co
   return 0;
 }
 
+int profile_common(grhd2_gpu_batch *b, float *ms, const char **names, int cap, int *n_out) {
+  cudaEvent_t start;
+  BCUDA_TRY(b, cudaEventCreate(&start));
+  BCUDA_TRY(b, cudaEventRecord(start, b->stream));
+  b->profiling = true;
+  int rc = refresh_batch(b);
+  if (!rc) rc = enqueue_step(b);
+  b->profiling = false;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  const int n = (int)b->prof_ev.size();
+  for (int k = 0; k < n; ++k) {
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, k == 0 ? start : b->prof_ev[k - 1], b->prof_ev[k]);
+    if (k < cap) {
+      if (ms) ms[k] = t;
+      if (names) names[k] = b->prof_names[k];
+    }
+  }
+  for (auto ev : b->prof_ev) cudaEventDestroy(ev);
+  cudaEventDestroy(start);
+  b->prof_ev.clear();
+  b->prof_names.clear();
+  if (n_out) *n_out = n;
+  if (rc) return rc;
+  if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "profile step: %s", cudaGetErrorString(e));
+  return GRHD2_OK;
+}
+
 }  // namespace
 
 // ======================================================================================
@@ -181,7 +376,7 @@ extern "C" {
 
 int grhd2_gpu_abi_version(void) { return GRHD2_GPU_ABI_VERSION; }
 
-int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out) {
+int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_gpu **out) {
   if (!cfg || !out) return GRHD2_ERR_ARG;
   *out = nullptr;
   grhd2_gpu *h = new (std::nothrow) grhd2_gpu();
@@ -205,14 +400,17 @@ int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out) {
   if (c.case_id == 5 && (c.nx < c.nghost || c.nz < c.nghost))
     return fail(h, GRHD2_ERR_ARG, "the jet's reflecting boundaries need nx, nz >= nghost");
   if (!(c.dx > 0) || (c.ny > 1 && !(c.dy > 0)) || (c.nz > 1 && !(c.dz > 0))) return fail(h, GRHD2_ERR_ARG, "grid spacing must be positive");
+  if ((long long)(c.nx + 1) * c.ny * c.nz > 2000000000LL || (long long)c.nx * (c.ny + 1) * c.nz > 2000000000LL ||
+      (long long)c.nx * c.ny * (c.nz + 1) > 2000000000LL)
+    return fail(h, GRHD2_ERR_ARG, "grid too large (face count must stay below 2e9)");
 
   h->mixed = c.precision_policy == GRHD2_PREC_MIXED;
-  h->phys.rec = c.rec_method; h->phys.lim = c.tvd_limiter; h->phys.rs = c.riemann; h->phys.sensor = c.shock_sensor ? 1 : 0;
-  h->phys.nonmink = c.metric_kind != GRHD2_METRIC_MINKOWSKI;
-  h->phys.srhd = c.metric_kind == GRHD2_METRIC_MINKOWSKI && c.geom_kind == GRHD2_GEOM_CARTESIAN;
-  h->phys.adb = c.adb_idx; h->phys.g1 = c.g1; h->phys.rho_floor = c.rho_floor; h->phys.p_floor = c.p_floor; h->phys.v_max = c.v_max;
-
   GridDev &G = h->G;
+  Phys &ph = G.phys;
+  ph.rec = c.rec_method; ph.lim = c.tvd_limiter; ph.rs = c.riemann; ph.sensor = c.shock_sensor ? 1 : 0;
+  ph.nonmink = c.metric_kind != GRHD2_METRIC_MINKOWSKI;
+  ph.srhd = c.metric_kind == GRHD2_METRIC_MINKOWSKI && c.geom_kind == GRHD2_GEOM_CARTESIAN;
+  ph.adb = c.adb_idx; ph.g1 = c.g1; ph.rho_floor = c.rho_floor; ph.p_floor = c.p_floor; ph.v_max = c.v_max;
   G.nx = c.nx; G.ny = c.ny; G.nz = c.nz; G.ng = c.nghost; G.case_id = c.case_id;
   G.ncell = (long long)c.nx * c.ny * c.nz;
   G.pplane = (G.ncell + 31) / 32 * 32;
@@ -221,21 +419,39 @@ int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out) {
   G.nface[1] = (long long)c.nx * (c.ny + 1);
   G.nface[2] = G.nij;
   G.rho_floor = c.rho_floor; G.p_floor = c.p_floor;
+  G.dx = c.dx; G.dy = c.dy; G.dz = c.dz;
 
   CUDA_TRY(h, cudaGetDevice(&h->device));
-  CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  if (stream) {
+    h->stream = (cudaStream_t)stream;
+  } else {
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
   int rc;
   const size_t es = h->mixed ? sizeof(float) : sizeof(double);
-  if ((rc = dalloc(h, (char **)&h->P, 5 * G.pplane * es))) return rc;
-  if ((rc = dalloc(h, &h->U, 5 * G.pplane))) return rc;
-  if ((rc = dalloc(h, &h->UP, 5 * G.pplane))) return rc;
-  const long long nfx = (long long)(c.nx + 1) * c.ny * c.nz;
-  if ((rc = dalloc(h, (char **)&h->F[0], 5 * nfx * es))) return rc;
-  if (c.ny > 1 && (rc = dalloc(h, (char **)&h->F[1], 5 * (long long)c.nx * (c.ny + 1) * c.nz * es))) return rc;
-  if (c.nz > 1 && (rc = dalloc(h, (char **)&h->F[2], 5 * (long long)c.nx * c.ny * (c.nz + 1) * es))) return rc;
-  if ((rc = dalloc(h, &h->cnt, NCNT))) return rc;
+  char *p = nullptr;
+  if ((rc = dalloc(h, &p, 5 * G.pplane * es))) return rc;
+  G.P = p;
+  if ((rc = dalloc(h, &G.U, 5 * G.pplane))) return rc;
+  if ((rc = dalloc(h, &G.UP, 5 * G.pplane))) return rc;
+  const long long nf[3] = {(long long)(c.nx + 1) * c.ny * c.nz, (long long)c.nx * (c.ny + 1) * c.nz,
+                           (long long)c.nx * c.ny * (c.nz + 1)};
+  long long nq = nf[0];
+  for (int d = 0; d < 3; ++d) {
+    if ((d == 1 && c.ny == 1) || (d == 2 && c.nz == 1)) continue;
+    nq = std::max(nq, nf[d]);
+    if ((rc = dalloc(h, &p, 5 * nf[d] * es))) return rc;
+    G.F[d] = p;
+  }
+  if ((rc = dalloc(h, &p, 10 * nq * es))) return rc;
+  G.Q = p;
+  if ((rc = dalloc(h, &G.cnt, NCNT))) return rc;
+  if ((rc = dalloc(h, &G.clock, 1))) return rc;
   if ((rc = dalloc(h, &h->red, 4))) return rc;
-  CUDA_TRY(h, cudaMemsetAsync(h->cnt, 0, NCNT * sizeof(unsigned long long), h->stream));
+  CUDA_TRY(h, cudaMemsetAsync(G.cnt, 0, NCNT * sizeof(unsigned long long), h->stream));
+  h->hclock = GridClock{0.0, 0.0, 0.0, 0.0, 0, -1, 0, 1};
+  if ((rc = write_clock(h))) return rc;
   h->n_ghosted = (size_t)5 * (c.nx + 2 * c.nghost + 1) * (c.ny + 2 * c.nghost + 1) * (c.nz + 2 * c.nghost + 1);
   h->n_interior = (size_t)5 * G.ncell;
   if ((rc = dalloc(h, &h->staging, h->n_ghosted))) return rc;
@@ -249,6 +465,8 @@ int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out) {
   h->err.clear();
   return GRHD2_OK;
 }
+
+int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out) { return grhd2_gpu_create_on_stream(cfg, nullptr, out); }
 
 int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m) {
   if (!h || !m) return GRHD2_ERR_ARG;
@@ -289,7 +507,6 @@ int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m) {
     for (int mu = 0; mu < 4; ++mu) C[(CF_DLNA + mu) * nij + q] = m->dlna_c[4 * q + mu];
     C[CF_VA * nij + q] = m->beta_c[3 * q] / m->alpha_c[q];
   }
-  // faces
   const double eps64 = 64.0 * DBL_EPSILON;
   std::vector<double> T[3];
   int rc;
@@ -308,8 +525,7 @@ int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m) {
     if ((rc = build_face_table(h, T[1], n, 2, m->alpha_f_y, m->beta_f_y, m->gamma_f_y, m->sqrt_gamma_f_y, zero))) return rc;
   }
   if (c.nz > 1) {
-    const size_t n = nij;
-    if ((rc = build_face_table(h, T[2], n, 3, m->alpha_f_z, m->beta_f_z, m->gamma_f_z, m->sqrt_gamma_f_z, {}))) return rc;
+    if ((rc = build_face_table(h, T[2], nij, 3, m->alpha_f_z, m->beta_f_z, m->gamma_f_z, m->sqrt_gamma_f_z, {}))) return rc;
   }
   if (!h->centre && (rc = dalloc(h, &h->centre, C.size()))) return rc;
   CUDA_TRY(h, cudaMemcpyAsync(h->centre, C.data(), C.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -323,6 +539,7 @@ int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m) {
   for (int d = 0; d < 3; ++d) h->G.face[d] = h->face[d];
   h->metric_set = true;
   h->dt_valid = false;
+  ++h->version;
   return GRHD2_OK;
 }
 
@@ -360,6 +577,7 @@ int grhd2_gpu_set_bc_data(grhd2_gpu *h, const grhd2_gpu_bc_view *b) {
   }
   for (int q = 0; q < 7; ++q) h->G.jet[q] = b->jet[q];
   h->bc_set = true;
+  ++h->version;
   return GRHD2_OK;
 }
 
@@ -370,17 +588,17 @@ int grhd2_gpu_upload(grhd2_gpu *h, const double *up, const double *p) {
   if (p) {
     CUDA_TRY(h, cudaMemcpyAsync(h->staging, p, h->n_ghosted * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     if (h->mixed)
-      k_prims_in<float><<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->staging, (float *)h->P, h->frozen[0],
-                                                                     G.ny > 0 ? h->frozen[1] : nullptr, h->frozen[2]);
+      k_prims_in<float><<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->staging, (float *)G.P, h->frozen[0],
+                                                                     h->frozen[1], h->frozen[2]);
     else
-      k_prims_in<double><<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->staging, (double *)h->P, h->frozen[0],
+      k_prims_in<double><<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->staging, (double *)G.P, h->frozen[0],
                                                                       h->frozen[1], h->frozen[2]);
     if (int rc = launch_check(h)) return rc;
     h->prims_set = true;
   }
   if (up) {
     CUDA_TRY(h, cudaMemcpyAsync(h->staging, up, h->n_interior * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    k_cons_in<<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->staging, h->UP);
+    k_cons_in<<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->staging, G.UP);
     if (int rc = launch_check(h)) return rc;
     h->cons_set = true;
   }
@@ -392,8 +610,8 @@ int grhd2_gpu_prim_to_cons_all(grhd2_gpu *h) {
   if (int rc = ready(h, false)) return rc;
   if (!h->prims_set) return fail(h, GRHD2_ERR_STATE, "primitives not uploaded");
   const GridDev &G = h->G;
-  if (h->mixed) k_p2c_all<float><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, h->phys, (const float *)h->P, h->UP);
-  else k_p2c_all<double><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, h->phys, (const double *)h->P, h->UP);
+  if (h->mixed) k_p2c_all<float><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (const float *)G.P, G.UP);
+  else k_p2c_all<double><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (const double *)G.P, G.UP);
   if (int rc = launch_check(h)) return rc;
   h->cons_set = true;
   return GRHD2_OK;
@@ -428,25 +646,40 @@ int grhd2_gpu_cfl(grhd2_gpu *h, double *dt_out) {
 
 int grhd2_gpu_step(grhd2_gpu *h, double dt) {
   if (int rc = ready(h, true)) return rc;
-  return step_dispatch(h, dt);
+  if (int rc = self_batch(h)) return rc;
+  h->hclock.mode = 0;
+  h->hclock.dt_explicit = dt;
+  if (int rc = write_clock(h)) return rc;
+  if (int rc = batch_steps(h->self, 1, false)) return fail(h, rc, "%s", h->self->err.c_str());
+  return GRHD2_OK;
 }
 
 int grhd2_gpu_run(grhd2_gpu *h, double t0, double final_time, int64_t max_steps, double *t_out, int64_t *steps_out) {
   if (int rc = ready(h, true)) return rc;
   double dt;
   if (int rc = grhd2_gpu_cfl(h, &dt)) return rc;
-  double t = t0;
-  int64_t n = 0;
-  while (t < final_time && (max_steps < 0 || n < max_steps)) {
-    double d = dt;
-    if (t + d > final_time) d = final_time - t;  // grhd2.f90:182-184
+  if (int rc = self_batch(h)) return rc;
+  // the host predicts the step count with the device clock's arithmetic (grhd2.f90:179-230)
+  GridClock c{t0, final_time, dt, 0.0, 0, max_steps, 1, 0};
+  c.active = t0 < final_time && max_steps != 0;
+  GridClock pred = c;
+  long long n = 0;
+  while (pred.active) {
+    pred.t = pred.t + clock_dt(pred);
+    pred.steps += 1;
+    pred.active = pred.t < pred.final_time && (pred.max_steps < 0 || pred.steps < pred.max_steps);
     ++n;
-    t = t + d;
-    if (int rc = step_dispatch(h, d)) return rc;
   }
+  h->hclock = c;
+  if (int rc = write_clock(h)) return rc;
+  if (int rc = batch_steps(h->self, n, true)) return fail(h, rc, "%s", h->self->err.c_str());
+  CUDA_TRY(h, cudaMemcpyAsync(&h->hclock, h->G.clock, sizeof(GridClock), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  if (t_out) *t_out = t;
-  if (steps_out) *steps_out = n;
+  if (h->hclock.steps != pred.steps || h->hclock.t != pred.t)
+    return fail(h, GRHD2_ERR_STATE, "device clock (%lld steps) differs from the host prediction (%lld)",
+                (long long)h->hclock.steps, (long long)pred.steps);
+  if (t_out) *t_out = h->hclock.t;
+  if (steps_out) *steps_out = h->hclock.steps;
   return GRHD2_OK;
 }
 
@@ -454,11 +687,21 @@ int grhd2_gpu_calc_rhs(grhd2_gpu *h, double *rhs_host) {
   if (int rc = ready(h, false)) return rc;
   if (!h->prims_set) return fail(h, GRHD2_ERR_STATE, "primitives not uploaded");
   int rc;
-  if (!h->RHS && (rc = dalloc(h, &h->RHS, 5 * h->G.pplane))) return rc;
-  if ((rc = h->mixed ? launch_fluxes<float, float>(h) : launch_fluxes<double, double>(h))) return rc;
-  if ((rc = h->mixed ? launch_update<0, float, float>(h, 0.0) : launch_update<0, double, double>(h, 0.0))) return rc;
+  if (!h->G.RHS) {
+    if ((rc = dalloc(h, &h->G.RHS, 5 * h->G.pplane))) return rc;
+    ++h->version;
+  }
+  if ((rc = self_batch(h))) return rc;
+  h->hclock.mode = 0;  // a finished run() leaves its clock inactive; the flux kernels would skip the grid
+  if ((rc = write_clock(h))) return rc;
+  grhd2_gpu_batch *b = h->self;
+  for (const auto &grp : b->groups) {
+    rc = grp.mixed ? enqueue_fluxes<float, float>(b, grp) : enqueue_fluxes<double, double>(b, grp);
+    if (!rc) rc = grp.mixed ? enqueue_cells<0, float, float>(b, grp) : enqueue_cells<0, double, double>(b, grp);
+    if (rc) return fail(h, rc, "%s", b->err.c_str());
+  }
   if (rhs_host) {
-    k_cons_out<<<nblocks(h->G.ncell, 256), 256, 0, h->stream>>>(h->G, h->RHS, h->staging);
+    k_cons_out<<<nblocks(h->G.ncell, 256), 256, 0, h->stream>>>(h->G, h->G.RHS, h->staging);
     if ((rc = launch_check(h))) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(rhs_host, h->staging, h->n_interior * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   }
@@ -470,8 +713,8 @@ int grhd2_gpu_cons_to_prim_all(grhd2_gpu *h) {
   if (int rc = ready(h, false)) return rc;
   if (!h->cons_set) return fail(h, GRHD2_ERR_STATE, "conserved state not uploaded");
   const GridDev &G = h->G;
-  if (h->mixed) k_c2p_all<float><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, h->phys, (float *)h->P, h->UP, h->cnt);
-  else k_c2p_all<double><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, h->phys, (double *)h->P, h->UP, h->cnt);
+  if (h->mixed) k_c2p_all<float><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (float *)G.P, G.UP, G.cnt);
+  else k_c2p_all<double><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (double *)G.P, G.UP, G.cnt);
   if (int rc = launch_check(h)) return rc;
   h->prims_set = true;
   return GRHD2_OK;
@@ -491,14 +734,14 @@ int grhd2_gpu_download(grhd2_gpu *h, double *up, double *p) {
     if (!h->prims_set) return fail(h, GRHD2_ERR_STATE, "primitives not uploaded");
     CUDA_TRY(h, cudaMemcpyAsync(h->staging, p, h->n_ghosted * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     const long long n = (long long)(G.nx + 2 * G.ng + 1) * (G.ny + 2 * G.ng + 1) * (G.nz + 2 * G.ng + 1);
-    if (h->mixed) k_prims_out<float><<<nblocks(n, 256), 256, 0, h->stream>>>(G, (const float *)h->P, h->staging);
-    else k_prims_out<double><<<nblocks(n, 256), 256, 0, h->stream>>>(G, (const double *)h->P, h->staging);
+    if (h->mixed) k_prims_out<float><<<nblocks(n, 256), 256, 0, h->stream>>>(G, (const float *)G.P, h->staging);
+    else k_prims_out<double><<<nblocks(n, 256), 256, 0, h->stream>>>(G, (const double *)G.P, h->staging);
     if (int rc = launch_check(h)) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(p, h->staging, h->n_ghosted * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   }
   if (up) {
     if (!h->cons_set) return fail(h, GRHD2_ERR_STATE, "conserved state not uploaded");
-    k_cons_out<<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->UP, h->staging);
+    k_cons_out<<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, G.UP, h->staging);
     if (int rc = launch_check(h)) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(up, h->staging, h->n_interior * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   }
@@ -510,7 +753,7 @@ int grhd2_gpu_get_counters(grhd2_gpu *h, grhd2_gpu_counters *out) {
   if (!h || !out) return GRHD2_ERR_ARG;
   CUDA_TRY(h, cudaSetDevice(h->device));
   unsigned long long c[NCNT];
-  CUDA_TRY(h, cudaMemcpyAsync(c, h->cnt, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(c, h->G.cnt, sizeof c, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   out->c2p_floor_pre = (int64_t)c[CNT_FLOOR_PRE];
   out->c2p_causal_rescale = (int64_t)c[CNT_CAUSAL];
@@ -526,7 +769,7 @@ int grhd2_gpu_get_counters(grhd2_gpu *h, grhd2_gpu_counters *out) {
 int grhd2_gpu_reset_counters(grhd2_gpu *h) {
   if (!h) return GRHD2_ERR_ARG;
   CUDA_TRY(h, cudaSetDevice(h->device));
-  CUDA_TRY(h, cudaMemsetAsync(h->cnt, 0, NCNT * sizeof(unsigned long long), h->stream));
+  CUDA_TRY(h, cudaMemsetAsync(h->G.cnt, 0, NCNT * sizeof(unsigned long long), h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return GRHD2_OK;
 }
@@ -547,9 +790,9 @@ static int faces_common(grhd2_gpu *h, int n, int dir, const double *qL, const do
   cudaMemcpy(dq, qL, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice);
   if (qR) cudaMemcpy(dq + 5 * n, qR, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice);
   if (h->mixed)
-    k_riemann_faces<float><<<nblocks(n, 128), 128>>>(h->phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n, physical_only);
+    k_riemann_faces<float><<<nblocks(n, 128), 128>>>(h->G.phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n, physical_only);
   else
-    k_riemann_faces<double><<<nblocks(n, 128), 128>>>(h->phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n, physical_only);
+    k_riemann_faces<double><<<nblocks(n, 128), 128>>>(h->G.phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n, physical_only);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpy(flux, dq + 10 * n, (size_t)5 * n * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(dT);
@@ -576,29 +819,11 @@ int grhd2_gpu_get_stream(grhd2_gpu *h, void **stream_out) {
 
 int grhd2_gpu_profile_step(grhd2_gpu *h, double dt, float *ms, const char **names, int cap, int *n_out) {
   if (int rc = ready(h, true)) return rc;
-  cudaEvent_t start;
-  CUDA_TRY(h, cudaEventCreate(&start));
-  CUDA_TRY(h, cudaEventRecord(start, h->stream));
-  h->profiling = true;
-  int rc = step_dispatch(h, dt);
-  h->profiling = false;
-  cudaError_t e = cudaStreamSynchronize(h->stream);
-  const int n = (int)h->prof_ev.size();
-  for (int k = 0; k < n; ++k) {
-    float t = 0.0f;
-    cudaEventElapsedTime(&t, k == 0 ? start : h->prof_ev[k - 1], h->prof_ev[k]);
-    if (k < cap) {
-      if (ms) ms[k] = t;
-      if (names) names[k] = h->prof_names[k];
-    }
-  }
-  for (auto ev : h->prof_ev) cudaEventDestroy(ev);
-  cudaEventDestroy(start);
-  h->prof_ev.clear();
-  h->prof_names.clear();
-  if (n_out) *n_out = n;
-  if (rc) return rc;
-  if (e != cudaSuccess) return fail(h, GRHD2_ERR_CUDA, "profile step: %s", cudaGetErrorString(e));
+  if (int rc = self_batch(h)) return rc;
+  h->hclock.mode = 0;
+  h->hclock.dt_explicit = dt;
+  if (int rc = write_clock(h)) return rc;
+  if (int rc = profile_common(h->self, ms, names, cap, n_out)) return fail(h, rc, "%s", h->self->err.c_str());
   return GRHD2_OK;
 }
 
@@ -615,11 +840,81 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *bufs[] = {h->P, h->U, h->UP, h->RHS, h->F[0], h->F[1], h->F[2], h->centre, h->face[0], h->face[1], h->face[2],
-                  h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1], h->frozen[2], h->cnt, h->red, h->staging};
+  if (h->self) {
+    destroy_batch_resources(h->self);
+    delete h->self;
+  }
+  void *bufs[] = {h->G.P, h->G.U, h->G.UP, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1], h->G.F[2], h->G.cnt, h->G.clock,
+                  h->centre, h->face[0], h->face[1], h->face[2], h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],
+                  h->frozen[2], h->red, h->staging};
   for (void *b : bufs) if (b) cudaFree(b);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
+}
+
+// ---- batches ---------------------------------------------------------------------------
+int grhd2_gpu_batch_create(grhd2_gpu **handles, int n, grhd2_gpu_batch **out) {
+  if (!handles || n <= 0 || !out) return GRHD2_ERR_ARG;
+  *out = nullptr;
+  grhd2_gpu_batch *b = new (std::nothrow) grhd2_gpu_batch();
+  if (!b) return GRHD2_ERR_NOMEM;
+  *out = b;
+  for (int k = 0; k < n; ++k) {
+    grhd2_gpu *h = handles[k];
+    if (!h) return bfail(b, GRHD2_ERR_ARG, "handle %d is NULL", k);
+    if (k > 0 && (h->device != b->device || h->stream != b->stream))
+      return bfail(b, GRHD2_ERR_ARG, "handle %d is on another device or stream (batched handles share one stream)", k);
+    if (!h->metric_set || !(h->prims_set && h->cons_set))
+      return bfail(b, GRHD2_ERR_STATE, "handle %d has no metric or state uploaded", k);
+    if ((h->cfg.case_id == 7 || h->cfg.case_id == 8 || h->cfg.case_id == 5) && !h->bc_set)
+      return bfail(b, GRHD2_ERR_STATE, "handle %d has no boundary data", k);
+    if (k == 0) { b->device = h->device; b->stream = h->stream; }
+    b->m.push_back(h);
+  }
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  return build_batch(b);
+}
+
+int grhd2_gpu_batch_set_clock(grhd2_gpu_batch *b, int k, double t0, double final_time, int64_t max_steps) {
+  if (!b || k < 0 || k >= (int)b->m.size()) return bfail(b, GRHD2_ERR_ARG, "grid index out of range");
+  grhd2_gpu *h = b->m[k];
+  double dt;
+  if (int rc = grhd2_gpu_cfl(h, &dt)) return bfail(b, rc, "grid %d: %s", k, h->err.c_str());
+  h->hclock = GridClock{t0, final_time, dt, 0.0, 0, max_steps, 1, (t0 < final_time && max_steps != 0) ? 1 : 0};
+  if (int rc = write_clock(h)) return bfail(b, rc, "%s", h->err.c_str());
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_batch_step(grhd2_gpu_batch *b, int nsteps, int use_graph) {
+  if (!b) return GRHD2_ERR_ARG;
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  return batch_steps(b, nsteps, use_graph != 0);
+}
+
+int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *steps, int *active) {
+  if (!b || k < 0 || k >= (int)b->m.size()) return bfail(b, GRHD2_ERR_ARG, "grid index out of range");
+  grhd2_gpu *h = b->m[k];
+  GridClock c;
+  BCUDA_TRY(b, cudaMemcpyAsync(&c, h->G.clock, sizeof c, cudaMemcpyDeviceToHost, b->stream));
+  BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  if (t) *t = c.t;
+  if (steps) *steps = c.steps;
+  if (active) *active = c.active;
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_batch_profile_step(grhd2_gpu_batch *b, float *ms, const char **names, int cap, int *n_out) {
+  if (!b) return GRHD2_ERR_ARG;
+  return profile_common(b, ms, names, cap, n_out);
+}
+
+const char *grhd2_gpu_batch_last_error(const grhd2_gpu_batch *b) { return b ? b->err.c_str() : "NULL batch"; }
+
+void grhd2_gpu_batch_destroy(grhd2_gpu_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  destroy_batch_resources(b);
+  delete b;
 }
 
 }  // extern "C"

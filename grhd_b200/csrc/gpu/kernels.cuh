@@ -1,8 +1,6 @@
 // kernels.cuh -- sm_100a kernels of the per-stage path.
 //
-//   face_flux<DIR>   one thread per face of direction DIR: stencil load with the boundary
-//                    fill evaluated on load, reconstruction (reconstruct_1d_core), Riemann
-//                    flux (resolve_riemann_problem); writes the face flux planes
+//   (face fluxes: flux.cuh)
 //   cell_update      one thread per cell: flux divergence + sources in calc_rhs's order,
 //                    SSP-RK3 stage combination (grhd2.f90:243-249) and con2prim
 //                    (equations.f90:94), or the bare RHS for grhd2_gpu_calc_rhs
@@ -11,42 +9,9 @@
 //   convert kernels  reference (Fortran AoS, ghosted) <-> device (SoA, interior) layouts
 #pragma once
 
-#include "state.cuh"
+#include "common.cuh"
 
 namespace grhd {
-
-enum CounterIdx { CNT_FLOOR_PRE = 0, CNT_CAUSAL, CNT_BRENT, CNT_ROOT_FAIL, CNT_BAD_V, CNT_SANITISE,
-                  CNT_RECON_CLAMP, CNT_HLLC_FALLBACK, NCNT };
-
-// warp-aggregated counter increment (call from converged code)
-__device__ __forceinline__ void count_add(unsigned long long *cnt, int idx, unsigned v) {
-  const unsigned mask = __activemask();
-  const unsigned tot = __reduce_add_sync(mask, v);
-  if (tot && (threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(&cnt[idx], (unsigned long long)tot);
-}
-
-template <class R>
-__device__ __forceinline__ FaceMetric<R> load_face_metric(const double *__restrict__ T, long long nf, long long f) {
-  FaceMetric<R> m;
-  m.alpha = R(__ldg(&T[FF_ALPHA * nf + f]));
-  m.beta_n = R(__ldg(&T[FF_BETA_N * nf + f]));
-  m.g11 = R(__ldg(&T[FF_G11 * nf + f])); m.g12 = R(__ldg(&T[FF_G12 * nf + f])); m.g13 = R(__ldg(&T[FF_G13 * nf + f]));
-  m.g22 = R(__ldg(&T[FF_G22 * nf + f])); m.g23 = R(__ldg(&T[FF_G23 * nf + f])); m.g33 = R(__ldg(&T[FF_G33 * nf + f]));
-  m.sqg = R(__ldg(&T[FF_SQG * nf + f]));
-  m.gup = R(__ldg(&T[FF_GUP * nf + f]));
-  return m;
-}
-template <class R>
-__device__ __forceinline__ FaceFrame<R> load_face_frame(const double *__restrict__ T, long long nf, long long f) {
-  FaceFrame<R> fr;
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int i = 0; i < 3; ++i) fr.cof[a][i] = R(__ldg(&T[(FF_COF + 3 * a + i) * nf + f]));
-  fr.gup = R(__ldg(&T[FF_GUP * nf + f]));
-  fr.ok = __ldg(&T[FF_FRAME_OK * nf + f]) != 0.0;
-  return fr;
-}
 
 // Riemann flux of one face given its interface states (resolve_riemann_problem)
 template <class R>
@@ -59,78 +24,6 @@ __device__ __forceinline__ bool riemann(const Phys &P, const R (&qL)[NEQ], const
   }
   hlle(P, qL, qR, dir, m, flux);
   return false;
-}
-
-// ------------------------------------------------------------------------------------
-// face flux kernel
-// ------------------------------------------------------------------------------------
-template <int DIR, class R, class PT>
-__global__ void __launch_bounds__(128) k_face_flux(const GridDev G, const Phys P, const PT *__restrict__ Pin,
-                                                   R *__restrict__ F, unsigned long long *__restrict__ cnt) {
-  const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
-  long long nfaces;
-  if (DIR == 1) nfaces = (long long)(G.nx + 1) * G.ny * G.nz;
-  else if (DIR == 2) nfaces = (long long)G.nx * (G.ny + 1) * G.nz;
-  else nfaces = (long long)G.nx * G.ny * (G.nz + 1);
-  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nfaces) return;
-  int i, j, k, face;  // i,j,k: 1-based cell indices of the strip; face: 0..n along DIR
-  long long ft;       // face-table index (k-invariant)
-  if (DIR == 1) {
-    face = (int)(f % (G.nx + 1)); const long long r = f / (G.nx + 1);
-    j = (int)(r % G.ny) + 1; k = (int)(r / G.ny) + 1; i = face;
-    ft = face + (long long)(G.nx + 1) * (j - 1);
-  } else if (DIR == 2) {
-    i = (int)(f % G.nx) + 1; const long long r = f / G.nx;
-    face = (int)(r % (G.ny + 1)); k = (int)(r / (G.ny + 1)) + 1; j = face;
-    ft = (i - 1) + (long long)G.nx * face;
-  } else {
-    i = (int)(f % G.nx) + 1; const long long r = f / G.nx;
-    j = (int)(r % G.ny) + 1; face = (int)(r / G.ny); k = face;
-    ft = (i - 1) + (long long)G.nx * (j - 1);
-  }
-  int lo, hi;
-  stencil_range(P.rec, P.sensor, lo, hi);
-  R w[NEQ][6];
-#pragma unroll
-  for (int m = 0; m < 6; ++m) {
-    if (m < lo || m > hi) {
-#pragma unroll
-      for (int v = 0; v < NEQ; ++v) w[v][m] = R(0);
-      continue;
-    }
-    double q[NEQ];
-    const int c = face - 2 + m;
-    if (DIR == 1) load_cell<1>(Pin, G, c, j, k, q);
-    else if (DIR == 2) load_cell<2>(Pin, G, i, c, k, q);
-    else load_cell<3>(Pin, G, i, j, c, q);
-#pragma unroll
-    for (int v = 0; v < NEQ; ++v) w[v][m] = R(q[v]);
-  }
-  const int br = recon_branch(P, w, face, n, DIR);
-  R qL[NEQ], qR[NEQ];
-#pragma unroll
-  for (int v = 0; v < NEQ; ++v) {
-    R s[6];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) s[m] = w[v][m];
-    recon_var(br, P.lim, s, qL[v], qR[v]);
-  }
-  const unsigned clamps = (unsigned)recon_floors(P, qL, qR);
-  const double *T = G.face[DIR - 1];
-  const long long nf = G.nface[DIR - 1];
-  R flux[NEQ];
-  bool fb = false;
-  if (__ldg(&T[FF_ZERO * nf + ft]) != 0.0) {
-#pragma unroll
-    for (int v = 0; v < NEQ; ++v) flux[v] = R(0);
-  } else {
-    fb = riemann(P, qL, qR, DIR, T, nf, ft, flux);
-  }
-#pragma unroll
-  for (int v = 0; v < NEQ; ++v) F[v * nfaces + f] = flux[v];
-  count_add(cnt, CNT_RECON_CLAMP, clamps);
-  if (P.rs == RS_HLLC) count_add(cnt, CNT_HLLC_FALLBACK, fb ? 1u : 0u);
 }
 
 // ------------------------------------------------------------------------------------
@@ -214,15 +107,29 @@ __device__ __forceinline__ void c2p_count(unsigned long long *cnt, unsigned fl) 
 // MODE 0 writes the RHS only; MODE 1..3 are the SSP-RK3 stages (stage 1 also copies
 // up into u, the "u = up" of grhd2.f90:232).
 // ------------------------------------------------------------------------------------
+// Batched: block b works on grid map[b].grid, cells map[b].first + threadIdx.x.
 template <int MODE, class R, class PT>
-__global__ void __launch_bounds__(128) k_cell_update(const GridDev G, const Phys P, PT *__restrict__ Pio,
-                                                     const R *__restrict__ Fx, const R *__restrict__ Fy,
-                                                     const R *__restrict__ Fz, double *__restrict__ U,
-                                                     double *__restrict__ UP, double *__restrict__ rhs_out,
-                                                     double dt, double dx, double dy, double dz,
-                                                     unsigned long long *__restrict__ cnt) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_cell_update(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+  const BlockMap bm = map[blockIdx.x];
+  const GridDev &G = grids[bm.grid];
+  const long long c = (long long)bm.first + threadIdx.x;
   if (c >= G.ncell) return;
+  const Phys P = G.phys;
+  PT *__restrict__ Pio = (PT *)G.P;
+  const R *__restrict__ Fx = (const R *)G.F[0];
+  const R *__restrict__ Fy = (const R *)G.F[1];
+  const R *__restrict__ Fz = (const R *)G.F[2];
+  double *__restrict__ U = G.U;
+  double *__restrict__ UP = G.UP;
+  double *__restrict__ rhs_out = G.RHS;
+  const double dx = G.dx, dy = G.dy, dz = G.dz;
+  double dt = 0.0;
+  if (MODE != 0) {
+    const GridClock ck = *G.clock;
+    if (clock_skip(ck)) return;
+    dt = clock_dt(ck);
+  }
+  unsigned long long *cnt = G.cnt;
   const int i0 = (int)(c % G.nx);
   const long long r = c / G.nx;
   const int j0 = (int)(r % G.ny), k0 = (int)(r / G.ny);
@@ -290,6 +197,22 @@ __global__ void __launch_bounds__(128) k_cell_update(const GridDev G, const Phys
     Pio[v * G.pplane + c] = (PT)pr[v];
   }
   c2p_count(cnt, fl);
+}
+
+// end of a step: t = t + dt, steps += 1 (grhd2.f90:229-230); deactivate grids that reached
+// their final time or step limit
+__global__ void k_advance_clocks(const GridDev *__restrict__ grids, int n) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  GridClock *c = grids[g].clock;
+  if (c->mode == 1) {
+    if (!c->active) return;
+    c->t = c->t + clock_dt(*c);
+    c->steps += 1;
+    c->active = c->t < c->final_time && (c->max_steps < 0 || c->steps < c->max_steps);
+  } else {
+    c->steps += 1;
+  }
 }
 
 template <class PT>

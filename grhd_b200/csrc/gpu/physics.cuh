@@ -176,91 +176,6 @@ __host__ __device__ __forceinline__ void stencil_range(int rec, int sensor, int 
   else { lo = 0; hi = 5; }
 }
 
-// reconstruct_1d_core branch selection for face i (reconstruction.f90:318-645).
-// w[v][m] = prim(v, i-2+m).
-template <class R>
-__device__ __forceinline__ int recon_branch(const Phys &P, const R (&w)[NEQ][6], int i, int nodes, int dir) {
-  R p_jump = R(0), rho_jump = R(0);
-  if (P.rec != REC_GODUNOV && P.sensor) {
-    R pmax = w[EQ_PR][0], pmin = w[EQ_PR][0], rmx = w[EQ_DE][0], rmn = w[EQ_DE][0];
-#pragma unroll
-    for (int m = 1; m < 5; ++m) {
-      pmax = rmax(pmax, w[EQ_PR][m]); pmin = rmin(pmin, w[EQ_PR][m]);
-      rmx = rmax(rmx, w[EQ_DE][m]); rmn = rmin(rmn, w[EQ_DE][m]);
-    }
-    const R pf = R(P.p_floor), rf = R(P.rho_floor);
-    p_jump = (pmax > R(1.0e3) * pf) ? (pmax - pmin) / rmax(pmin, pf) : R(0);
-    rho_jump = (rmx > R(1.0e3) * rf) ? (rmx - rmn) / rmax(rmn, rf) : R(0);
-  }
-  const bool inner = P.nonmink && dir == 1 && i <= 0;
-  const R atm = R(1.0e2) * R(P.rho_floor);
-  const bool atmo = w[EQ_DE][2] <= atm || w[EQ_DE][3] <= atm;
-  const bool cliff = p_jump >= R(10.0) || rho_jump >= R(10.0);
-  const bool shock = p_jump >= R(0.80) || rho_jump >= R(0.50);
-  const bool smooth_break = p_jump >= R(0.40) || rho_jump >= R(0.15);
-  switch (P.rec) {
-    case REC_GODUNOV: return BR_GODUNOV;
-    case REC_TVD:
-      if (P.sensor && (inner || atmo || cliff)) return BR_GODUNOV;
-      return BR_TVD;
-    case REC_WENO3:
-      if (P.sensor) {
-        if (inner || atmo || cliff) return BR_GODUNOV;
-        if (shock) return BR_TVD_MC;
-        return BR_WENO3;
-      }
-      return inner ? BR_GODUNOV : BR_WENO3;
-    case REC_MP5:
-      if (P.sensor) {
-        if (inner || atmo || cliff) return BR_GODUNOV;
-        if (shock) return BR_TVD_MC;
-        if (smooth_break || (P.nonmink && dir == 1 && i <= 3) ||
-            (P.nonmink && dir == 2 && (i <= 2 || i >= nodes - 2)))
-          return BR_WENO3;
-        return BR_MP5;
-      }
-      return inner ? BR_GODUNOV : BR_MP5;
-    default:
-      if (P.sensor) {
-        if (inner || atmo || cliff) return BR_GODUNOV;
-        if (shock) return BR_TVD_MC;
-        if (smooth_break) return BR_WENO3;
-        return BR_WENO5;
-      }
-      return inner ? BR_GODUNOV : BR_WENO5;
-  }
-}
-
-// interface states of one variable for a branch
-template <class R>
-__device__ __forceinline__ void recon_var(int br, int lim, const R (&s)[6], R &qL, R &qR) {
-  switch (br) {
-    case BR_GODUNOV: qL = s[2]; qR = s[3]; break;
-    case BR_TVD:
-    case BR_TVD_MC: {
-      const int l = (br == BR_TVD) ? lim : LIM_MC;
-      qL = s[2] + R(0.5) * tvd_slope(s[2] - s[1], s[3] - s[2], l);
-      qR = s[3] - R(0.5) * tvd_slope(s[3] - s[2], s[4] - s[3], l);
-      break;
-    }
-    case BR_WENO3: qL = weno3(s[1], s[2], s[3]); qR = weno3(s[4], s[3], s[2]); break;
-    case BR_MP5: qL = mp5(s[0], s[1], s[2], s[3], s[4]); qR = mp5(s[5], s[4], s[3], s[2], s[1]); break;
-    default: qL = weno5(s[0], s[1], s[2], s[3], s[4]); qR = weno5(s[5], s[4], s[3], s[2], s[1]); break;
-  }
-}
-
-// reconstruction.f90:647-655 positivity floors; returns the number of values raised
-template <class R>
-__device__ __forceinline__ int recon_floors(const Phys &P, R (&qL)[NEQ], R (&qR)[NEQ]) {
-  const R rf = R(P.rho_floor), pf = R(P.p_floor);
-  int n = 0;
-  n += !(qL[EQ_DE] >= rf); qL[EQ_DE] = rmax(qL[EQ_DE], rf);
-  n += !(qR[EQ_DE] >= rf); qR[EQ_DE] = rmax(qR[EQ_DE], rf);
-  n += !(qL[EQ_PR] >= pf); qL[EQ_PR] = rmax(qL[EQ_PR], pf);
-  n += !(qR[EQ_PR] >= pf); qR[EQ_PR] = rmax(qR[EQ_PR], pf);
-  return n;
-}
-
 // ------------------------------------------------------------------------------------
 // equations.f90:434-502, fluxes.f90:76-156, 669-803
 // ------------------------------------------------------------------------------------
@@ -452,10 +367,12 @@ __device__ __forceinline__ bool local_to_coord(const R (&ul)[NEQ], const R (&fl)
   return true;
 }
 
-// calc_hllc_fluxes, fluxes.f90:174-397.  Returns true when it fell back to HLLE.
+// calc_hllc_fluxes, fluxes.f90:174-397, without its HLLE exits: returns true when the
+// reference would fall back to calc_hlle_fluxes (the caller then runs HLLE, so a kernel
+// holds one copy of the HLLE code).
 template <class R>
-__device__ bool hllc(const Phys &P, const R (&qL)[NEQ], const R (&qR)[NEQ], int dir,
-                     const FaceMetric<R> &m, const FaceFrame<R> &fr, R (&flux)[NEQ]) {
+__device__ bool hllc_try(const Phys &P, const R (&qL)[NEQ], const R (&qR)[NEQ], int dir,
+                         const FaceMetric<R> &m, const FaceFrame<R> &fr, R (&flux)[NEQ]) {
   const R alpha = m.alpha, sqg = m.sqg;
   R qLh[NEQ], qRh[NEQ], uL[NEQ], uR[NEQ], fL[NEQ], fR[NEQ];
   R lLmin, lLmax, lRmin, lRmax;
@@ -566,8 +483,16 @@ __device__ bool hllc(const Phys &P, const R (&qL)[NEQ], const R (&qR)[NEQ], int 
     return false;
   }
 fallback:
-  hlle(P, qL, qR, dir, m, flux);
   return true;
+}
+
+// calc_hllc_fluxes with its HLLE exits; returns true when it fell back
+template <class R>
+__device__ __forceinline__ bool hllc(const Phys &P, const R (&qL)[NEQ], const R (&qR)[NEQ], int dir,
+                                     const FaceMetric<R> &m, const FaceFrame<R> &fr, R (&flux)[NEQ]) {
+  const bool fb = hllc_try(P, qL, qR, dir, m, fr, flux);
+  if (fb) hlle(P, qL, qR, dir, m, flux);
+  return fb;
 }
 
 // ------------------------------------------------------------------------------------
@@ -603,7 +528,7 @@ __device__ __forceinline__ void residual(double g1, double W, double D, double t
 }
 // equations.f90:343-424 (per-call locals reproduce the reference: its SAVE'd d, e are
 // written in the first iteration before being read)
-__device__ double root_brent(double g1, double rho_floor, double D, double tau, double Q2) {
+__device__ inline double root_brent(double g1, double rho_floor, double D, double tau, double Q2) {
   const double EPS = 3.0e-8, x_acc = 1.0e-8, x1 = 1.0;
   const double Wg = (sqrt(Q2) + D) / rmax(D, rho_floor);
   const double x2 = rmax(1.0e4, Wg * 2.0);
@@ -638,7 +563,7 @@ __device__ double root_brent(double g1, double rho_floor, double D, double tau, 
   return -1.0;
 }
 // equations.f90:249-340
-__device__ double root_safe_newton(double g1, double rho_floor, double D, double tau, double Q2, unsigned &flags) {
+__device__ inline double root_safe_newton(double g1, double rho_floor, double D, double tau, double Q2, unsigned &flags) {
   const double x_acc = 1.0e-10, x1 = 1.0;
   const double Wg = (sqrt(Q2) + D) / rmax(D, rho_floor);
   const double x2 = rmax(1.0e3, Wg * 2.0);
@@ -675,7 +600,7 @@ __device__ double root_safe_newton(double g1, double rho_floor, double D, double
 }
 
 // cons_to_prim, equations.f90:94-205: cons modified in place (intent(inout)); returns flags
-__device__ unsigned cons_to_prim(const Phys &P, const CellMetric &m, double (&cs)[NEQ], double (&pr)[NEQ]) {
+__device__ inline unsigned cons_to_prim(const Phys &P, const CellMetric &m, double (&cs)[NEQ], double (&pr)[NEQ]) {
   unsigned flags = 0;
   const double lDf = P.rho_floor * m.sqg;
   const double lTf = P.p_floor * (P.g1 - 1.0) * m.sqg;

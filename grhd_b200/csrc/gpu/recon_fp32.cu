@@ -1,0 +1,6 @@
+// recon_fp32.cu -- reconstruction kernels, float instantiation (see flux.cuh).
+#include "flux_launch.cuh"
+
+namespace grhd {
+template void launch_recon<float, float>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
+}  // namespace grhd

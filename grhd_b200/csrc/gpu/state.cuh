@@ -45,6 +45,23 @@ __host__ __device__ __forceinline__ int sym4(int mu, int nu) {
   return mu == 0 ? nu : (mu == 1 ? 3 + nu : (mu == 2 ? 5 + nu : 9));
 }
 
+// Per-grid time keeping on the device.  mode 0: the caller passes dt (grhd2_gpu_step);
+// mode 1: the grid steps with its CFL dt clamped to its final time (grhd2.f90:180-184)
+// and deactivates when it reaches it, so steps of a batch can be replayed as one graph
+// without host involvement.
+struct GridClock {
+  double t, final_time, dt_cfl, dt_explicit;
+  long long steps, max_steps;
+  int mode, active;
+};
+__host__ __device__ __forceinline__ double clock_dt(const GridClock &c) {
+  if (c.mode == 0) return c.dt_explicit;
+  return (c.t + c.dt_cfl > c.final_time) ? c.final_time - c.t : c.dt_cfl;
+}
+__host__ __device__ __forceinline__ bool clock_skip(const GridClock &c) { return c.mode == 1 && !c.active; }
+
+// Everything a kernel needs about one grid.  The stage kernels read these descriptors from
+// a device array, one entry per grid of a batch (a single grid is a batch of one).
 struct GridDev {
   // sizes
   int nx, ny, nz, ng;
@@ -63,6 +80,21 @@ struct GridDev {
   const double *frozen[3];  // -nghost slabs [v][..] (nghost == 2 only)
   double jet[7];
   double rho_floor, p_floor;
+  // physics of the grid (adiabatic index, floors, limiter, sensor, metric flags)
+  Phys phys;
+  double dx, dy, dz;
+  // the grid's device state
+  void *P;                      // primitives (double or float planes)
+  double *U, *UP, *RHS;         // conserved u, up; RHS scratch of grhd2_gpu_calc_rhs
+  void *F[3];                   // face fluxes per direction
+  void *Q;                      // interface states of the direction being processed
+  unsigned long long *cnt;      // failure / floor counters
+  GridClock *clock;             // device clock of the grid
+};
+
+// one block of a batched launch: the grid it works on and its first item (face or cell)
+struct BlockMap {
+  int grid, first;
 };
 
 // interior primitive read (1-based cell indices)

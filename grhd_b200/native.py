@@ -96,6 +96,16 @@ GPU_SYMBOLS = {
     "grhd2_gpu_last_error": (C.c_char_p, [_VP]),
     "grhd2_gpu_destroy": (None, [_VP]),
     "grhd2_gpu_abi_version": (C.c_int, []),
+    "grhd2_gpu_create_on_stream": (C.c_int, [C.POINTER(GpuConfig), _VP, C.POINTER(_VP)]),
+    "grhd2_gpu_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(_VP)]),
+    "grhd2_gpu_batch_set_clock": (C.c_int, [_VP, C.c_int, C.c_double, C.c_double, C.c_int64]),
+    "grhd2_gpu_batch_step": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "grhd2_gpu_batch_get_clock": (C.c_int, [_VP, C.c_int, c_double_p, C.POINTER(C.c_int64),
+                                            C.POINTER(C.c_int)]),
+    "grhd2_gpu_batch_profile_step": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_char_p),
+                                               C.c_int, C.POINTER(C.c_int)]),
+    "grhd2_gpu_batch_last_error": (C.c_char_p, [_VP]),
+    "grhd2_gpu_batch_destroy": (None, [_VP]),
 }
 
 HOST_SYMBOLS = {

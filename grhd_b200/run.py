@@ -1,0 +1,130 @@
+"""Command-line runner: advance a problem on the GPU (the device-side counterpart of
+``./grhd2 file.par`` without I/O) and report device time per SSP-RK3 step.
+
+    python -m grhd_b200.run --par case.par [--steps N] [--precision fp64|mixed]
+    python -m grhd_b200.run --workload torus3d --nx 128 --ny 64 --nz 64 --steps 4
+
+Workloads name the benchmark configurations (shock tube, Michel, 2.5D and 3D Kerr-Schild
+tori); extra ``--key value`` pairs override .par keys.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+
+WORKLOADS = {
+    "shock": ("sod", dict(nx=400, adiabatic_index=1.6666666666666667, sod_density_left=10,
+                          sod_pressure_left=13.33, sod_density_right=1, sod_pressure_right=1e-6,
+                          reconstruction="weno5", riemann_solver="hlle", cfl=0.4, final_time=0.4)),
+    "michel": ("michel", dict(metric="eddington_finkelstein", geometry="spherical", logarithmic_r=True,
+                              bh_mass=1.0, nx=1024, ny=1, nz=1, r_min=1.8, r_max=20.0,
+                              adiabatic_index=1.3333333333333333, michel_critical_radius=8.0,
+                              reconstruction="mp5", riemann_solver="hlle", final_time=500.0,
+                              perturbation="density_noise", perturbation_amplitude=0.001,
+                              perturbation_time=0.0, perturbation_seed=3435)),
+    "torus2p5d": ("fishbone_equatorial", dict(
+        metric="kerr_schild", geometry="spheroidal", logarithmic_r=True, spin=0.9, bh_mass=1.0, nx=400,
+        ny=1, nz=200, r_min=1.2, r_max=40.0, theta_min=0, theta_max=1, phi_min=0, phi_max=2,
+        fm_inner_radius=6.0, fm_pressure_max_radius=12.0, fm_polytropic_constant=0.0015,
+        adiabatic_index=1.3333333333333333, reconstruction="weno5", riemann_solver="hlle",
+        shock_sensor=False, cfl=0.4, perturbation="pressure_noise", perturbation_amplitude=0.01,
+        perturbation_time=0.0, perturbation_seed=3435)),
+    "torus3d": ("fishbone_3d", dict(
+        metric="kerr_schild", geometry="spheroidal", logarithmic_r=True, spin=0.9, bh_mass=1.0, nx=256,
+        ny=128, nz=128, r_min=1.2, r_max=40.0, theta_min=0, theta_max=1, phi_min=0, phi_max=2,
+        fm_inner_radius=6.0, fm_pressure_max_radius=12.0, fm_polytropic_constant=0.0015,
+        adiabatic_index=1.3333333333333333, reconstruction="mp5", riemann_solver="hllc",
+        shock_sensor=True, cfl=0.4, perturbation="pressure_noise", perturbation_amplitude=0.01,
+        perturbation_time=0.0, perturbation_seed=3435)),
+}
+
+
+def workload_text(name: str, **overrides) -> str:
+    from .problem import par_text
+    problem, keys = WORKLOADS[name]
+    keys = dict(keys)
+    keys.update(overrides)
+    return par_text(problem, **keys)
+
+
+def with_key(text: str, key: str, value) -> str:
+    """.par text with every assignment of key replaced by key = value."""
+    keep = [ln for ln in text.splitlines() if ln.split("=")[0].strip().lower() != key]
+    return "\n".join(keep + [f"{key} = {value}"]) + "\n"
+
+
+def _parse_overrides(rest):
+    out = {}
+    it = iter(rest)
+    for k in it:
+        if not k.startswith("--"):
+            raise SystemExit(f"unexpected argument {k}")
+        v = next(it)
+        out[k[2:].replace("-", "_")] = v
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--par", help=".par file")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS))
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--batch", type=int, default=1, help="replicas stepped as one batch")
+    ap.add_argument("--graph", type=int, default=1, help="replay each step as a CUDA graph")
+    args, rest = ap.parse_known_args(argv)
+    overrides = _parse_overrides(rest)
+    from .problem import Problem
+    from .solver import GpuBatch, GpuGrid
+    if args.par:
+        text = open(args.par).read()
+        for k, v in overrides.items():
+            text += f"{k} = {v}\n"
+    elif args.workload:
+        text = workload_text(args.workload, **overrides)
+    else:
+        raise SystemExit("give --par or --workload")
+    pb = Problem(text)
+    p = pb.initial_prims()
+    if pb.info.perturbation_type and pb.info.perturbation_time <= 0.0:
+        pb.perturb(p)
+    # replicas of the problem, each with its own perturbation seed, on one stream
+    grids = []
+    for r in range(max(1, args.batch)):
+        pr = pb if r == 0 else Problem(with_key(text, "perturbation_seed", 3435 + r))
+        q = p
+        if r > 0:
+            q = pr.initial_prims()
+            if pr.info.perturbation_type and pr.info.perturbation_time <= 0.0:
+                pr.perturb(q)
+        gr = GpuGrid(pr, precision=args.precision, upload_initial=False,
+                     stream=grids[0].stream_ptr if grids else None)
+        gr.upload(p=q)
+        gr.prim_to_cons()
+        grids.append(gr)
+    g = grids[0]
+    batch = GpuBatch(grids)
+    for k in range(len(grids)):
+        batch.set_clock(k, 0.0, 1e300, -1)
+    batch.step(args.warmup, graph=args.graph)
+    g.synchronize()
+    t0 = time.perf_counter()
+    batch.step(args.steps, graph=args.graph)
+    g.synchronize()
+    el = time.perf_counter() - t0
+    prof = batch.profile_step()
+    cells = pb.n_cells * len(grids)
+    out = {"cells": cells, "grids": len(grids), "steps": args.steps, "dt": g.cfl(),
+           "ms_per_step": el / args.steps * 1e3, "zone_updates_per_s": cells * args.steps / el,
+           "kernels": prof, "counters": g.counters()}
+    batch.close()
+    for gr in reversed(grids):
+        gr.close()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

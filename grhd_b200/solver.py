@@ -28,7 +28,10 @@ class GpuError(RuntimeError):
 class GpuGrid:
     """One grid on the GPU, built from a :class:`Problem` (or explicit config/tables)."""
 
-    def __init__(self, problem: Problem, precision: str = "fp64", upload_initial: bool = True):
+    def __init__(self, problem: Problem, precision: str = "fp64", upload_initial: bool = True,
+                 stream: int | None = None):
+        """stream: a cudaStream_t (integer) the handle launches on; None creates a private
+        one.  Grids that will step together in a :class:`GpuBatch` share one stream."""
         self.lib = N.gpu_lib()
         self.problem = problem
         self.precision = precision
@@ -36,7 +39,10 @@ class GpuGrid:
         self._mv = problem.metric_view()
         self._bv = problem.bc_view()
         h = C.c_void_p()
-        rc = self.lib.grhd2_gpu_create(C.byref(self.cfg), C.byref(h))
+        if stream is None:
+            rc = self.lib.grhd2_gpu_create(C.byref(self.cfg), C.byref(h))
+        else:
+            rc = self.lib.grhd2_gpu_create_on_stream(C.byref(self.cfg), C.c_void_p(stream), C.byref(h))
         self._h = h
         self._check(rc)
         self._check(self.lib.grhd2_gpu_set_metric(self._h, C.byref(self._mv)))
@@ -176,6 +182,68 @@ class GpuGrid:
         self._check(self.lib.grhd2_gpu_physical_flux(self._h, n, dir, N.dptr(q), N.dptr(alpha), N.dptr(beta),
                                                      N.dptr(gamma), N.dptr(sqg), N.dptr(flux)))
         return flux
+
+
+class GpuBatch:
+    """Many grids stepped together: one launch per kernel kind and scheme group, so grids
+    of uneven sizes fill the GPU together; a step can replay as one CUDA graph.  Each grid
+    keeps its own clock (t, final time, CFL dt) on the device and stops by itself when it
+    reaches its final time or step limit."""
+
+    def __init__(self, grids: list[GpuGrid]):
+        self.lib = N.gpu_lib()
+        self.grids = list(grids)
+        arr = (C.c_void_p * len(self.grids))(*[g._h.value for g in self.grids])
+        b = C.c_void_p()
+        rc = self.lib.grhd2_gpu_batch_create(arr, len(self.grids), C.byref(b))
+        self._b = b
+        self._check(rc)
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self.lib.grhd2_gpu_batch_last_error(self._b) if self._b else b"batch create failed"
+            raise GpuError(rc, (msg or b"").decode())
+
+    def close(self):
+        if getattr(self, "_b", None) is not None and self._b.value:
+            self.lib.grhd2_gpu_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_clock(self, k: int, t0: float, final_time: float, max_steps: int = -1):
+        """Grid k runs from t0 to final_time (at most max_steps steps, -1 unlimited) with its
+        CFL dt clamped to the final time, as the time loop of grhd2.f90:179-230."""
+        self._check(self.lib.grhd2_gpu_batch_set_clock(self._b, k, t0, final_time, max_steps))
+
+    def step(self, nsteps: int = 1, graph: bool = True):
+        """Enqueue nsteps batched steps (asynchronous)."""
+        self._check(self.lib.grhd2_gpu_batch_step(self._b, nsteps, 1 if graph else 0))
+
+    def clock(self, k: int):
+        """(t, steps, active) of grid k (synchronises the stream)."""
+        t, n, a = C.c_double(), C.c_int64(), C.c_int()
+        self._check(self.lib.grhd2_gpu_batch_get_clock(self._b, k, C.byref(t), C.byref(n), C.byref(a)))
+        return t.value, n.value, bool(a.value)
+
+    def profile_step(self):
+        """[(kernel name, ms)] for every launch of one batched step."""
+        cap = 256
+        ms = (C.c_float * cap)()
+        names = (C.c_char_p * cap)()
+        n = C.c_int()
+        self._check(self.lib.grhd2_gpu_batch_profile_step(self._b, ms, names, cap, C.byref(n)))
+        return [(names[k].decode(), float(ms[k])) for k in range(min(n.value, cap))]
 
 
 def l1_relative(a: np.ndarray, b: np.ndarray) -> np.ndarray:

@@ -148,6 +148,32 @@ int grhd2_gpu_physical_flux(grhd2_gpu *h, int n, int dir, const double *q, const
                             double *flux);
 /* Wait for all work of the handle; returns the first asynchronous error. */
 int grhd2_gpu_synchronize(grhd2_gpu *h);
+
+/* ---- batched grids (no reference counterpart) ---------------------------------------
+ * The reference runs independent problems as separate processes
+ * (inundaciones.sh:542-548).  Here independent grids -- any sizes, schemes, metrics and
+ * boundary cases -- advance together: one launch per kernel kind covers every grid of the
+ * batch that uses the same scheme, Riemann solver and precision, and a whole step can be
+ * replayed as one CUDA graph.  Each grid keeps its own clock: it steps with its CFL dt,
+ * clamped to its final time (grhd2.f90:182-184), and stops when it reaches it. */
+typedef struct grhd2_gpu_batch grhd2_gpu_batch;
+/* Like grhd2_gpu_create, but the handle works on the caller's CUDA stream (a cudaStream_t;
+ * NULL creates a private stream).  Handles that will be batched must share one stream. */
+int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_gpu **out);
+/* Group n handles (same device and stream, metric and state uploaded). */
+int grhd2_gpu_batch_create(grhd2_gpu **handles, int n, grhd2_gpu_batch **out);
+/* Set grid k's clock: time t0, final time, and a step limit (< 0: none).  The CFL dt is
+ * computed from the grid's metric (update_adaptive_dt). */
+int grhd2_gpu_batch_set_clock(grhd2_gpu_batch *b, int k, double t0, double final_time, int64_t max_steps);
+/* Advance every grid that has not reached its final time by up to nsteps steps (one CUDA
+ * graph per step when use_graph != 0).  Asynchronous; grids that finish early stop. */
+int grhd2_gpu_batch_step(grhd2_gpu_batch *b, int nsteps, int use_graph);
+/* Read grid k's clock (synchronises the stream). */
+int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *steps, int *active);
+/* Per-launch timing of one batched step (names/ms as in grhd2_gpu_profile_step). */
+int grhd2_gpu_batch_profile_step(grhd2_gpu_batch *b, float *ms, const char **names, int cap, int *n_out);
+const char *grhd2_gpu_batch_last_error(const grhd2_gpu_batch *b);
+void grhd2_gpu_batch_destroy(grhd2_gpu_batch *b);
 /* The handle's CUDA stream (a cudaStream_t) so callers can order their own work and
  * record timing events on it.  No reference counterpart (the reference has no device). */
 int grhd2_gpu_get_stream(grhd2_gpu *h, void **stream_out);
