@@ -2,34 +2,42 @@
 // that depends only on the face metric: the Cramer gamma^dd used by
 // calc_wavespeeds_grhd (fluxes.f90:760-774) and the orthonormal face frame of
 // build_face_orthonormal_frame (fluxes.f90:402-473).  Evaluated once per face on the host
-// when the metric tables are uploaded; same arithmetic, same order, IEEE double.
+// when the metric tables are uploaded; same arithmetic, same order, IEEE double.  The
+// functions also compile for the device (the allocation-free face entry point builds its
+// per-face table there).
 #pragma once
 
 #include <cmath>
 
+#if defined(__CUDACC__)
+#define GRHD_HD __host__ __device__
+#else
+#define GRHD_HD
+#endif
+
 namespace grhd {
 
 // g: Fortran (3,3) array g[(a-1)+3(b-1)]
-inline double det3(const double *g) {
+GRHD_HD inline double det3(const double *g) {
 #define GA(a, b) g[((a) - 1) + 3 * ((b) - 1)]
   return GA(1, 1) * (GA(2, 2) * GA(3, 3) - GA(2, 3) * GA(3, 2)) - GA(1, 2) * (GA(2, 1) * GA(3, 3) - GA(2, 3) * GA(3, 1)) +
          GA(1, 3) * (GA(2, 1) * GA(3, 2) - GA(2, 2) * GA(3, 1));
 }
 // gamma^dd of calc_wavespeeds_grhd
-inline double gamma_up_dd(const double *g, int dir) {
+GRHD_HD inline double gamma_up_dd(const double *g, int dir) {
   const double det = det3(g);
   if (dir == 1) return (GA(2, 2) * GA(3, 3) - GA(2, 3) * GA(3, 2)) / det;
   if (dir == 2) return (GA(1, 1) * GA(3, 3) - GA(1, 3) * GA(3, 1)) / det;
   return (GA(1, 1) * GA(2, 2) - GA(1, 2) * GA(2, 1)) / det;
 }
-inline double metric_dot3(const double *a, const double *b, const double *g) {
+GRHD_HD inline double metric_dot3(const double *a, const double *b, const double *g) {
   double s = 0.0;
   for (int i = 1; i <= 3; ++i)
     for (int j = 1; j <= 3; ++j) s = s + GA(i, j) * a[i - 1] * b[j - 1];
   return s;
 }
 // cof[3a+i] = coframe(a+1,i+1); returns ok
-inline bool face_frame(const double *g, int dir, double *cof, double *gup) {
+GRHD_HD inline bool face_frame(const double *g, int dir, double *cof, double *gup) {
   double frame[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int q = 0; q < 9; ++q) cof[q] = 0.0;
   *gup = 0.0;

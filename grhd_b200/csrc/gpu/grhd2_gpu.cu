@@ -22,6 +22,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -809,6 +810,109 @@ int grhd2_gpu_riemann_faces(grhd2_gpu *h, int n, int dir, const double *qL, cons
 int grhd2_gpu_physical_flux(grhd2_gpu *h, int n, int dir, const double *q, const double *alpha, const double *beta,
                             const double *gamma, const double *sqg, double *flux) {
   return faces_common(h, n, dir, q, nullptr, alpha, beta, gamma, sqg, flux, 1);
+}
+
+}  // extern "C"
+
+// ---- allocation-free face fluxes ------------------------------------------------------
+// Scratch of grhd2_gpu_riemann_faces_noalloc: one fixed array per device, laid out as
+// regions of GRHD2_GPU_NOALLOC_MAX_FACES entries (faces of one call are indexed 0..n-1 in
+// each region).  Every region is written by the call before it is read, so nothing needs
+// to start at zero.
+namespace {
+constexpr size_t NA_MAX = GRHD2_GPU_NOALLOC_MAX_FACES;
+constexpr size_t NA_ALPHA = 0, NA_BETA = NA_ALPHA + NA_MAX, NA_GAMMA = NA_BETA + 3 * NA_MAX,
+                 NA_SQG = NA_GAMMA + 9 * NA_MAX, NA_TABLE = NA_SQG + NA_MAX, NA_QL = NA_TABLE + NFF * NA_MAX,
+                 NA_QR = NA_QL + 5 * NA_MAX, NA_FLUX = NA_QR + 5 * NA_MAX, NA_TOTAL = NA_FLUX + 5 * NA_MAX;
+static_assert(NA_TOTAL == 50 * NA_MAX, "50 doubles per face");
+
+static __device__ __align__(256) double g_noalloc_scratch[NA_TOTAL];
+
+constexpr int NA_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[NA_MAX_DEVICES] = {};
+
+// per-face table of n faces (the fields build_face_table writes), built on the device
+__global__ void k_face_table(int n, int dir, const double *__restrict__ alpha, const double *__restrict__ beta,
+                             const double *__restrict__ gamma, const double *__restrict__ sqg, double *__restrict__ T) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n) return;
+  double g[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) g[q] = gamma[9 * f + q];
+  const size_t m = (size_t)n;
+  T[FF_ALPHA * m + f] = alpha[f];
+  T[FF_BETA_N * m + f] = beta[3 * f + (dir - 1)];
+  T[FF_G11 * m + f] = g[0]; T[FF_G12 * m + f] = g[3]; T[FF_G13 * m + f] = g[6];
+  T[FF_G22 * m + f] = g[4]; T[FF_G23 * m + f] = g[7]; T[FF_G33 * m + f] = g[8];
+  T[FF_SQG * m + f] = sqg[f];
+  T[FF_GUP * m + f] = gamma_up_dd(g, dir);
+  double cof[9], gup;
+  const bool ok = face_frame(g, dir, cof, &gup);
+#pragma unroll
+  for (int q = 0; q < 9; ++q) T[(FF_COF + q) * m + f] = cof[q];
+  T[FF_FRAME_OK * m + f] = ok ? 1.0 : 0.0;
+  T[FF_ZERO * m + f] = 0.0;
+}
+
+// device address of the scratch on the handle's device (looked up once per device)
+int noalloc_scratch(grhd2_gpu *h, double **out) {
+  if (h->device < 0 || h->device >= NA_MAX_DEVICES)
+    return fail(h, GRHD2_ERR_ARG, "device %d is beyond the %d devices the allocation-free entry supports", h->device,
+                NA_MAX_DEVICES);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[h->device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(h, GRHD2_ERR_CUDA, "cudaGetSymbolAddress of the face scratch: %s", cudaGetErrorString(e));
+    g_noalloc_ptr[h->device] = (double *)p;
+  }
+  *out = g_noalloc_ptr[h->device];
+  return GRHD2_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int grhd2_gpu_riemann_faces_noalloc(grhd2_gpu *h, int n, int dir, const double *qL, const double *qR,
+                                    const double *alpha, const double *beta, const double *gamma, const double *sqg,
+                                    double *flux) {
+  if (!h || n < 0 || dir < 1 || dir > 3 || !qL || !qR || !alpha || !beta || !gamma || !sqg || !flux)
+    return fail(h, GRHD2_ERR_ARG, "invalid arguments to the allocation-free face-flux entry point");
+  if ((size_t)n > NA_MAX)
+    return fail(h, GRHD2_ERR_ARG, "%d faces exceed the allocation-free scratch (at most %d faces per call)", n,
+                GRHD2_GPU_NOALLOC_MAX_FACES);
+  if (n == 0) return GRHD2_OK;
+  for (int f = 0; f < n; ++f) {
+    const double *g = &gamma[9 * (size_t)f];
+    if (!bit_equal(g[1], g[3]) || !bit_equal(g[2], g[6]) || !bit_equal(g[5], g[7]))
+      return fail(h, GRHD2_ERR_ARG, "face metric of direction %d is not exactly symmetric at face %d", dir, f);
+  }
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  double *s = nullptr;
+  if (int rc = noalloc_scratch(h, &s)) return rc;
+  const size_t m = (size_t)n;
+  cudaStream_t st = h->stream;
+  CUDA_TRY(h, cudaMemcpyAsync(s + NA_ALPHA, alpha, m * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(s + NA_BETA, beta, 3 * m * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(s + NA_GAMMA, gamma, 9 * m * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(s + NA_SQG, sqg, m * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(s + NA_QL, qL, 5 * m * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(s + NA_QR, qR, 5 * m * sizeof(double), cudaMemcpyHostToDevice, st));
+  k_face_table<<<nblocks(n, 128), 128, 0, st>>>(n, dir, s + NA_ALPHA, s + NA_BETA, s + NA_GAMMA, s + NA_SQG,
+                                                s + NA_TABLE);
+  if (int rc = launch_check(h)) return rc;
+  if (h->mixed)
+    k_riemann_faces<float><<<nblocks(n, 128), 128, 0, st>>>(h->G.phys, n, dir, s + NA_QL, s + NA_QR, s + NA_TABLE,
+                                                            s + NA_FLUX, 0);
+  else
+    k_riemann_faces<double><<<nblocks(n, 128), 128, 0, st>>>(h->G.phys, n, dir, s + NA_QL, s + NA_QR, s + NA_TABLE,
+                                                             s + NA_FLUX, 0);
+  if (int rc = launch_check(h)) return rc;
+  CUDA_TRY(h, cudaMemcpyAsync(flux, s + NA_FLUX, 5 * m * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  return GRHD2_OK;
 }
 
 int grhd2_gpu_get_stream(grhd2_gpu *h, void **stream_out) {

@@ -87,6 +87,9 @@ GPU_SYMBOLS = {
     "grhd2_gpu_riemann_faces": (C.c_int, [_VP, C.c_int, C.c_int, c_double_p, c_double_p,
                                           c_double_p, c_double_p, c_double_p, c_double_p,
                                           c_double_p]),
+    "grhd2_gpu_riemann_faces_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, c_double_p, c_double_p,
+                                                  c_double_p, c_double_p, c_double_p, c_double_p,
+                                                  c_double_p]),
     "grhd2_gpu_physical_flux": (C.c_int, [_VP, C.c_int, C.c_int, c_double_p, c_double_p,
                                           c_double_p, c_double_p, c_double_p, c_double_p]),
     "grhd2_gpu_synchronize": (C.c_int, [_VP]),

@@ -171,6 +171,20 @@ class GpuGrid:
                                                      N.dptr(beta), N.dptr(gamma), N.dptr(sqg), N.dptr(flux)))
         return flux
 
+    def riemann_faces_noalloc(self, dir: int, qL, qR, alpha, beta, gamma, sqg) -> np.ndarray:
+        """riemann_faces through the allocation-free entry point: the library allocates
+        nothing (fixed device scratch of GRHD2_GPU_NOALLOC_MAX_FACES faces; more raises)."""
+        qL, qR = (np.ascontiguousarray(a, dtype=np.float64) for a in (qL, qR))
+        n = qL.shape[0]
+        alpha, sqg = (np.ascontiguousarray(np.broadcast_to(a, (n,)), dtype=np.float64) for a in (alpha, sqg))
+        beta = np.ascontiguousarray(np.broadcast_to(beta, (n, 3)), dtype=np.float64)
+        gamma = np.ascontiguousarray(np.broadcast_to(gamma, (n, 3, 3)).transpose(0, 2, 1), dtype=np.float64)
+        flux = np.empty((n, 5))
+        self._check(self.lib.grhd2_gpu_riemann_faces_noalloc(
+            self._h, n, dir, N.dptr(qL), N.dptr(qR), N.dptr(alpha), N.dptr(beta), N.dptr(gamma), N.dptr(sqg),
+            N.dptr(flux)))
+        return flux
+
     def physical_flux(self, dir: int, q, alpha, beta, gamma, sqg) -> np.ndarray:
         """calc_fluxes (equations.f90:434) for n states."""
         q = np.ascontiguousarray(q, dtype=np.float64)

@@ -142,6 +142,26 @@ int grhd2_gpu_reset_counters(grhd2_gpu *h);
 int grhd2_gpu_riemann_faces(grhd2_gpu *h, int n, int dir, const double *qL, const double *qR,
                             const double *alpha, const double *beta, const double *gamma,
                             const double *sqg, double *flux);
+/* Allocation-free variant of grhd2_gpu_riemann_faces (no counterpart in the reference):
+ * same arguments, same results, but it never allocates memory, on the device or the host.
+ * grhd2_gpu_riemann_faces allocates device buffers on every call; a caller that runs
+ * under a fixed memory budget (the device memory is already handed out to a caching
+ * allocator or to resident grids), or that must not stall other streams (cudaMalloc and
+ * cudaFree can synchronise the whole device), can use this one instead.
+ *  - Scratch is one fixed device array in the library, GRHD2_GPU_NOALLOC_MAX_FACES faces
+ *    of 50 doubles each (6.6 MB).  n > GRHD2_GPU_NOALLOC_MAX_FACES returns GRHD2_ERR_ARG.
+ *  - Nothing in the scratch has to start at zero: each call writes every element it
+ *    later reads.
+ *  - The first call on a device looks up the scratch address (cudaGetSymbolAddress) and
+ *    caches it; make that first call before any stream capture.
+ *  - The scratch is shared by every handle of a device: calls made at the same time from
+ *    several host threads on the same device race on it.  Serialise them.
+ * The call copies and launches on the handle's stream and returns after the flux is on
+ * the host. */
+#define GRHD2_GPU_NOALLOC_MAX_FACES 16384
+int grhd2_gpu_riemann_faces_noalloc(grhd2_gpu *h, int n, int dir, const double *qL, const double *qR,
+                                    const double *alpha, const double *beta, const double *gamma,
+                                    const double *sqg, double *flux);
 /* Physical flux F(q) for n states (calc_fluxes, equations.f90:434). */
 int grhd2_gpu_physical_flux(grhd2_gpu *h, int n, int dir, const double *q, const double *alpha,
                             const double *beta, const double *gamma, const double *sqg,
