@@ -62,6 +62,17 @@ def build_host(force=False, verbose=False) -> str:
     return out
 
 
+def _precision_flags(src: str):
+    """FP64 translation units keep every multiply and add separately rounded (the parity
+    path follows the reference's operation order).  The *_fp32.cu units hold only the
+    single-precision reconstruction and Riemann kernels of the mixed policy, whose bar is
+    an L1 tolerance, not bitwise parity: they contract to FMA and use the approximate
+    single-precision division and square root."""
+    if src.endswith("_fp32.cu"):
+        return ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
+    return ["--fmad=false"]
+
+
 def build_gpu(force=False, verbose=False) -> str:
     """Each .cu compiles to its own object in parallel, then one shared library links them.
     --fmad=false keeps every multiply and add separately rounded (the FP64 parity path
@@ -74,14 +85,14 @@ def build_gpu(force=False, verbose=False) -> str:
     headers = _sources("gpu", (".cuh", ".h")) + [os.path.join(INCLUDE, "grhd2_gpu.h")]
     if not srcs:
         raise RuntimeError("no CUDA sources under grhd_b200/csrc/gpu")
-    common = [_nvcc()] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
+    common = [_nvcc()] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                                  "-I" + INCLUDE, "-I" + os.path.join(CSRC, "gpu"), "-ccbin", _cxx()]
     objs, jobs = [], []
     for s in srcs:
         o = os.path.join(obj_dir, os.path.splitext(os.path.basename(s))[0] + ".o")
         objs.append(o)
         if force or _newer(o, [s] + headers):
-            jobs.append(common + ["-c", "-o", o, s])
+            jobs.append(common + _precision_flags(s) + ["-c", "-o", o, s])
     if jobs:
         from concurrent.futures import ThreadPoolExecutor
         with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:

@@ -25,22 +25,26 @@ struct FaceIndex {
 };
 
 template <int DIR>
-__device__ __forceinline__ FaceIndex decode_face(const GridDev &G, long long f) {
+__device__ __forceinline__ FaceIndex decode_face(const GridDev &G, long long f64) {
   FaceIndex x;
+  const unsigned f = (unsigned)f64;  // < 2^31 faces per grid
   if (DIR == 1) {
-    x.face = (int)(f % (G.nx + 1));
-    const long long r = f / (G.nx + 1);
-    x.j = (int)(r % G.ny) + 1; x.k = (int)(r / G.ny) + 1; x.i = x.face;
+    const unsigned r = fdiv(f, G.div_nx1);
+    x.face = (int)(f - r * G.div_nx1.d);
+    const unsigned k = fdiv(r, G.div_ny);
+    x.j = (int)(r - k * G.div_ny.d) + 1; x.k = (int)k + 1; x.i = x.face;
     x.ft = x.face + (long long)(G.nx + 1) * (x.j - 1);
   } else if (DIR == 2) {
-    x.i = (int)(f % G.nx) + 1;
-    const long long r = f / G.nx;
-    x.face = (int)(r % (G.ny + 1)); x.k = (int)(r / (G.ny + 1)) + 1; x.j = x.face;
+    const unsigned r = fdiv(f, G.div_nx);
+    x.i = (int)(f - r * G.div_nx.d) + 1;
+    const unsigned k = fdiv(r, G.div_ny1);
+    x.face = (int)(r - k * G.div_ny1.d); x.k = (int)k + 1; x.j = x.face;
     x.ft = (x.i - 1) + (long long)G.nx * x.face;
   } else {
-    x.i = (int)(f % G.nx) + 1;
-    const long long r = f / G.nx;
-    x.j = (int)(r % G.ny) + 1; x.face = (int)(r / G.ny); x.k = x.face;
+    const unsigned r = fdiv(f, G.div_nx);
+    x.i = (int)(f - r * G.div_nx.d) + 1;
+    const unsigned k = fdiv(r, G.div_ny);
+    x.j = (int)(r - k * G.div_ny.d) + 1; x.face = (int)k; x.k = x.face;
     x.ft = (x.i - 1) + (long long)G.nx * (x.j - 1);
   }
   return x;
@@ -135,8 +139,18 @@ __device__ __forceinline__ void recon_one(int br, int lim, const R (&s)[6], R &q
 
 // Batched launches: block b works on grid map[b].grid, faces map[b].first + threadIdx.x.
 // Q layout per grid: Q[(side*5 + v) * nfaces + f], side 0 = q_L, 1 = q_R
+// Resident blocks per SM the register allocation must allow (256-thread recon blocks,
+// 128-thread Riemann blocks).  Both kernels stall on dependent FP64 chains, so occupancy
+// pays more than the few registers it costs: measured on the batched 2.5D torus and the
+// 3D torus, 4 recon blocks (64 registers) and 8 Riemann blocks (64 registers) are fastest.
+#ifndef GRHD_RECON_MIN_BLOCKS
+#define GRHD_RECON_MIN_BLOCKS 4
+#endif
+#ifndef GRHD_RIEMANN_MIN_BLOCKS
+#define GRHD_RIEMANN_MIN_BLOCKS 8
+#endif
 template <int DIR, int REC, class R, class PT>
-__global__ void __launch_bounds__(256) k_recon(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+__global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;
@@ -151,17 +165,29 @@ __global__ void __launch_bounds__(256) k_recon(const GridDev *__restrict__ grids
   const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
   int lo, hi;
   stencil_range(REC, P.sensor, lo, hi);
+  // a stencil entirely inside the grid reads P directly at a fixed stride along DIR
+  const bool inside = x.face - 2 + lo >= 1 && x.face - 2 + hi <= n;
+  const long long stride = DIR == 1 ? 1LL : (DIR == 2 ? (long long)G.nx : (long long)G.nx * G.ny);
+  long long base = 0;
+  if (inside) {
+    const int c0 = x.face - 2 + lo;
+    base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
+  }
+  auto ld = [&](int w, int m) -> R {
+    return inside ? R((double)__ldg(&Pin[w * G.pplane + base + m * stride]))
+                  : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, w));
+  };
   R s[6];
 #pragma unroll
-  for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? R(load_var<DIR>(Pin, G, x, x.face - 2 + m, v)) : R(0);
+  for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ld(v, m) : R(0);
   int br = BR_GODUNOV;
   if (REC != REC_GODUNOV) {
     R rho[5], pr[5];
     if (P.sensor) {
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        rho[m] = v == EQ_DE ? s[m] : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, EQ_DE));
-        pr[m] = v == EQ_PR ? s[m] : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, EQ_PR));
+        rho[m] = v == EQ_DE ? s[m] : ld(EQ_DE, m);
+        pr[m] = v == EQ_PR ? s[m] : ld(EQ_PR, m);
       }
     } else {
 #pragma unroll
@@ -183,8 +209,96 @@ __global__ void __launch_bounds__(256) k_recon(const GridDev *__restrict__ grids
   count_add(cnt, CNT_RECON_CLAMP, clamps);
 }
 
+// ------------------------------------------------------------------------------------
+// Fused alternative: one thread per face reconstructs all five variables and solves the
+// Riemann problem, so q_L, q_R never leave the SM.  Same arithmetic as k_recon + k_riemann
+// (bit-identical results); the branch of the sensor cascade is evaluated once per face
+// instead of once per (face, variable).  The variable loop is kept rolled (one copy of
+// the reconstruction code) and the interface states are staged in shared memory.
+// ------------------------------------------------------------------------------------
+constexpr int FLUX_BS = 128;
+
+template <int DIR, int REC, int RS, class R, class PT>
+__global__ void __launch_bounds__(FLUX_BS) k_flux(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+  __shared__ R sq[2 * NEQ][FLUX_BS];
+  const BlockMap bm = map[blockIdx.x];
+  const GridDev &G = grids[bm.grid];
+  const Phys P = G.phys;
+  const long long nf = n_faces<DIR>(G);
+  const long long f = (long long)bm.first + threadIdx.x;
+  if (f >= nf || clock_skip(*G.clock)) return;
+  const PT *__restrict__ Pin = (const PT *)G.P;
+  const FaceIndex x = decode_face<DIR>(G, f);
+  const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
+  int lo, hi;
+  stencil_range(REC, P.sensor, lo, hi);
+  // a stencil entirely inside the grid reads P directly at a fixed stride along DIR
+  const bool inside = x.face - 2 + lo >= 1 && x.face - 2 + hi <= n;
+  const long long stride = DIR == 1 ? 1LL : (DIR == 2 ? (long long)G.nx : (long long)G.nx * G.ny);
+  long long base = 0;
+  if (inside) {
+    const int c0 = x.face - 2 + lo;
+    base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
+  }
+  auto ld = [&](int v, int m) -> R {
+    return inside ? R((double)__ldg(&Pin[v * G.pplane + base + m * stride]))
+                  : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, v));
+  };
+  int br = BR_GODUNOV;
+  if (REC != REC_GODUNOV) {
+    R rho[5], pr[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      rho[m] = P.sensor ? ld(EQ_DE, m) : R(0);
+      pr[m] = P.sensor ? ld(EQ_PR, m) : R(0);
+    }
+    br = branch_of<REC>(P, rho, pr, x.face, n, DIR);
+  }
+  unsigned clamps = 0;
+#pragma unroll 1
+  for (int v = 0; v < NEQ; ++v) {
+    R s[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ld(v, m) : R(0);
+    R qL, qR;
+    recon_one<REC>(br, P.lim, s, qL, qR);
+    if (v == EQ_DE || v == EQ_PR) {  // reconstruction.f90:647-655
+      const R fl = v == EQ_DE ? R(P.rho_floor) : R(P.p_floor);
+      clamps += (unsigned)!(qL >= fl) + (unsigned)!(qR >= fl);
+      qL = rmax(qL, fl);
+      qR = rmax(qR, fl);
+    }
+    sq[v][threadIdx.x] = qL;
+    sq[NEQ + v][threadIdx.x] = qR;
+  }
+  count_add(G.cnt, CNT_RECON_CLAMP, clamps);
+  R qL[NEQ], qR[NEQ], flux[NEQ];
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) { qL[v] = sq[v][threadIdx.x]; qR[v] = sq[NEQ + v][threadIdx.x]; }
+  R *__restrict__ F = (R *)G.F[DIR - 1];
+  const double *T = G.face[DIR - 1];
+  const long long ntab = G.nface[DIR - 1];
+  bool fb = false;
+  if (__ldg(&T[FF_ZERO * ntab + x.ft]) != 0.0) {
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) flux[v] = R(0);
+  } else {
+    const FaceMetric<R> m = load_face_metric<R>(T, ntab, x.ft);
+    if (RS == RS_HLLC) {
+      const FaceFrame<R> fr = load_face_frame<R>(T, ntab, x.ft);
+      fb = hllc_try(P, qL, qR, DIR, m, fr, flux);
+    } else {
+      fb = true;
+    }
+    if (fb) hlle(P, qL, qR, DIR, m, flux);
+  }
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) F[(long long)v * nf + f] = flux[v];
+  if (RS == RS_HLLC) count_add(G.cnt, CNT_HLLC_FALLBACK, fb ? 1u : 0u);
+}
+
 template <int DIR, int RS, class R>
-__global__ void __launch_bounds__(128) k_riemann(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+__global__ void __launch_bounds__(128, GRHD_RIEMANN_MIN_BLOCKS) k_riemann(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;

@@ -1,0 +1,6 @@
+// flux_fp64_y.cu -- fused face-flux kernels of direction y, double instantiation (see flux.cuh).
+#include "flux_launch.cuh"
+
+namespace grhd {
+template void launch_flux_dir<2, double, double>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
+}  // namespace grhd

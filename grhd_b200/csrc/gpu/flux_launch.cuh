@@ -43,4 +43,23 @@ void launch_riemann(int dir, int rs, const GridDev *grids, const BlockMap *map, 
   }
 }
 
+template <int DIR, int REC, class R, class PT>
+inline void flux_rs(int rs, const GridDev *grids, const BlockMap *map, unsigned nb, cudaStream_t s) {
+  if (rs == RS_HLLC) k_flux<DIR, REC, RS_HLLC, R, PT><<<nb, FLUX_BS, 0, s>>>(grids, map);
+  else k_flux<DIR, REC, RS_HLLE, R, PT><<<nb, FLUX_BS, 0, s>>>(grids, map);
+}
+
+template <int DIR, class R, class PT>
+void launch_flux_dir(int rec, int rs, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
+  if (nblocks <= 0) return;
+  const unsigned nb = (unsigned)nblocks;
+  switch (rec) {
+    case REC_GODUNOV: flux_rs<DIR, REC_GODUNOV, R, PT>(rs, grids, map, nb, s); break;
+    case REC_TVD: flux_rs<DIR, REC_TVD, R, PT>(rs, grids, map, nb, s); break;
+    case REC_WENO3: flux_rs<DIR, REC_WENO3, R, PT>(rs, grids, map, nb, s); break;
+    case REC_MP5: flux_rs<DIR, REC_MP5, R, PT>(rs, grids, map, nb, s); break;
+    default: flux_rs<DIR, REC_WENO5, R, PT>(rs, grids, map, nb, s); break;
+  }
+}
+
 }  // namespace grhd

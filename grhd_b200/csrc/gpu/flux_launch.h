@@ -13,11 +13,34 @@ struct BlockMap;
 constexpr int RECON_BS = 256;
 constexpr int RIEMANN_BS = 128;
 constexpr int CELL_BS = 128;
+constexpr int FUSED_FLUX_BS = 128;  // k_flux (flux.cuh FLUX_BS)
 
 template <class R, class PT>
 void launch_recon(int dir, int rec, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
 template <class R>
 void launch_riemann(int dir, int rs, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
+
+template <int DIR, class R, class PT>
+void launch_flux_dir(int rec, int rs, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
+
+#define GRHD_FLUX_EXTERN(D, R, PT) \
+  extern template void launch_flux_dir<D, R, PT>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
+GRHD_FLUX_EXTERN(1, double, double)
+GRHD_FLUX_EXTERN(2, double, double)
+GRHD_FLUX_EXTERN(3, double, double)
+GRHD_FLUX_EXTERN(1, float, float)
+GRHD_FLUX_EXTERN(2, float, float)
+GRHD_FLUX_EXTERN(3, float, float)
+#undef GRHD_FLUX_EXTERN
+
+// fused face fluxes of direction dir (recon + Riemann in one kernel)
+template <class R, class PT>
+inline void launch_flux(int dir, int rec, int rs, const GridDev *grids, const BlockMap *map, int nblocks,
+                        cudaStream_t s) {
+  if (dir == 1) launch_flux_dir<1, R, PT>(rec, rs, grids, map, nblocks, s);
+  else if (dir == 2) launch_flux_dir<2, R, PT>(rec, rs, grids, map, nblocks, s);
+  else launch_flux_dir<3, R, PT>(rec, rs, grids, map, nblocks, s);
+}
 
 extern template void launch_recon<double, double>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
 extern template void launch_recon<float, float>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);

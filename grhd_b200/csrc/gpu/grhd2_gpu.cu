@@ -22,7 +22,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <new>
 #include <string>
 #include <vector>
@@ -44,13 +46,17 @@ int vfail(std::string &err, int code, const char *fmt, va_list ap) {
 }
 
 // kernel kinds of a step and their items-per-block
-enum Kind { K_RECON_X = 0, K_RIEMANN_X, K_RECON_Y, K_RIEMANN_Y, K_RECON_Z, K_RIEMANN_Z, K_CELL, NKIND };
-const int KIND_BS[NKIND] = {RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, CELL_BS};
-const char *KIND_NAME[NKIND] = {"recon_x", "riemann_x", "recon_y", "riemann_y", "recon_z", "riemann_z", "cell_update"};
+enum Kind {
+  K_RECON_X = 0, K_RIEMANN_X, K_RECON_Y, K_RIEMANN_Y, K_RECON_Z, K_RIEMANN_Z, K_CELL, K_FLUX_X, K_FLUX_Y, K_FLUX_Z, NKIND
+};
+const int KIND_BS[NKIND] = {RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, CELL_BS,
+                            FUSED_FLUX_BS, FUSED_FLUX_BS, FUSED_FLUX_BS};
+const char *KIND_NAME[NKIND] = {"recon_x", "riemann_x", "recon_y", "riemann_y", "recon_z", "riemann_z",
+                                "cell_update", "flux_x", "flux_y", "flux_z"};
 
 long long kind_items(const GridDev &G, int k) {
   if (k == K_CELL) return G.ncell;
-  const int dir = k / 2 + 1;
+  const int dir = k >= K_FLUX_X ? k - K_FLUX_X + 1 : k / 2 + 1;
   if (dir == 2 && G.ny == 1) return 0;
   if (dir == 3 && G.nz == 1) return 0;
   if (dir == 1) return (long long)(G.nx + 1) * G.ny * G.nz;
@@ -92,6 +98,7 @@ struct Group {
   std::vector<int> members;
   BlockMap *d_map = nullptr;
   int off[NKIND], nb[NKIND];
+  int variant[3];  // per direction: GRHD2_FLUX_SPLIT or GRHD2_FLUX_FUSED
 };
 
 struct grhd2_gpu_batch {
@@ -101,6 +108,7 @@ struct grhd2_gpu_batch {
   cudaStream_t stream = nullptr;
   GridDev *d_grids = nullptr;
   std::vector<Group> groups;
+  int variant_request = GRHD2_FLUX_AUTO;  // GRHD2_FLUX_AUTO: tuned choice if cached, else the default
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool profiling = false;
@@ -176,6 +184,38 @@ void destroy_batch_resources(grhd2_gpu_batch *b) {
   b->d_grids = nullptr;
 }
 
+// ---- flux variant choice --------------------------------------------------------------
+// Tuned choices are cached per process, keyed by what decides the winner: precision,
+// scheme, Riemann solver, shock sensor, direction and the size class of the launch
+// (log2 of the faces in the group).
+struct TuneKey {
+  int mixed, rec, rs, sensor, dir, size_class;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(mixed, rec, rs, sensor, dir, size_class) <
+           std::tie(o.mixed, o.rec, o.rs, o.sensor, o.dir, o.size_class);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+
+TuneKey tune_key(const Group &grp, const std::vector<GridDev> &hg, int dir) {
+  long long faces = 0;
+  for (int g : grp.members) faces += kind_items(hg[g], 2 * (dir - 1));
+  int cls = 0;
+  while ((1LL << (cls + 1)) <= faces) ++cls;
+  return TuneKey{grp.mixed ? 1 : 0, grp.rec, grp.rs, hg[grp.members[0]].phys.sensor, dir, cls};
+}
+
+// default without tuning: the split kernels (recon at high occupancy, lean Riemann)
+constexpr int DEFAULT_VARIANT = GRHD2_FLUX_SPLIT;
+
+int choose_variant(const grhd2_gpu_batch *b, const Group &grp, const std::vector<GridDev> &hg, int dir) {
+  if (b->variant_request == GRHD2_FLUX_SPLIT || b->variant_request == GRHD2_FLUX_FUSED) return b->variant_request;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tune.find(tune_key(grp, hg, dir));
+  return it == g_tune.end() ? DEFAULT_VARIANT : it->second;
+}
+
 // (re)build device descriptors and block maps of a batch
 int build_batch(grhd2_gpu_batch *b) {
   destroy_batch_resources(b);
@@ -191,7 +231,7 @@ int build_batch(grhd2_gpu_batch *b) {
     for (auto &x : b->groups)
       if (x.mixed == h->mixed && x.rec == h->cfg.rec_method && x.rs == h->cfg.riemann) grp = &x;
     if (!grp) {
-      b->groups.push_back(Group{h->mixed, h->cfg.rec_method, h->cfg.riemann, {}, nullptr, {}, {}});
+      b->groups.push_back(Group{h->mixed, h->cfg.rec_method, h->cfg.riemann, {}, nullptr, {}, {}, {0, 0, 0}});
       grp = &b->groups.back();
     }
     grp->members.push_back(g);
@@ -206,6 +246,7 @@ int build_batch(grhd2_gpu_batch *b) {
       }
       grp.nb[k] = (int)map.size() - grp.off[k];
     }
+    for (int d = 0; d < 3; ++d) grp.variant[d] = choose_variant(b, grp, hg, d + 1);
     BCUDA_TRY(b, cudaMalloc((void **)&grp.d_map, sizeof(BlockMap) * std::max<size_t>(1, map.size())));
     BCUDA_TRY(b, cudaMemcpyAsync(grp.d_map, map.data(), sizeof(BlockMap) * map.size(), cudaMemcpyHostToDevice, b->stream));
   }
@@ -221,18 +262,30 @@ int refresh_batch(grhd2_gpu_batch *b) {
 
 // kind 0..5 for directions, then the cell kernel in MODE (0 rhs, 1..3 stages)
 template <class R, class PT>
-int enqueue_fluxes(grhd2_gpu_batch *b, const Group &grp) {
-  for (int d = 1; d <= 3; ++d) {
-    const int kr = 2 * (d - 1), ks = kr + 1;
-    if (grp.nb[kr] > 0) {
-      launch_recon<R, PT>(d, grp.rec, b->d_grids, grp.d_map + grp.off[kr], grp.nb[kr], b->stream);
-      if (int rc = blaunch_check(b, KIND_NAME[kr])) return rc;
+int enqueue_dir(grhd2_gpu_batch *b, const Group &grp, int d, int variant) {
+  const int kr = 2 * (d - 1), ks = kr + 1, kf = K_FLUX_X + d - 1;
+  if (variant == GRHD2_FLUX_FUSED) {
+    if (grp.nb[kf] > 0) {
+      launch_flux<R, PT>(d, grp.rec, grp.rs, b->d_grids, grp.d_map + grp.off[kf], grp.nb[kf], b->stream);
+      if (int rc = blaunch_check(b, KIND_NAME[kf])) return rc;
     }
-    if (grp.nb[ks] > 0) {
-      launch_riemann<R>(d, grp.rs, b->d_grids, grp.d_map + grp.off[ks], grp.nb[ks], b->stream);
-      if (int rc = blaunch_check(b, KIND_NAME[ks])) return rc;
-    }
+    return 0;
   }
+  if (grp.nb[kr] > 0) {
+    launch_recon<R, PT>(d, grp.rec, b->d_grids, grp.d_map + grp.off[kr], grp.nb[kr], b->stream);
+    if (int rc = blaunch_check(b, KIND_NAME[kr])) return rc;
+  }
+  if (grp.nb[ks] > 0) {
+    launch_riemann<R>(d, grp.rs, b->d_grids, grp.d_map + grp.off[ks], grp.nb[ks], b->stream);
+    if (int rc = blaunch_check(b, KIND_NAME[ks])) return rc;
+  }
+  return 0;
+}
+
+template <class R, class PT>
+int enqueue_fluxes(grhd2_gpu_batch *b, const Group &grp) {
+  for (int d = 1; d <= 3; ++d)
+    if (int rc = enqueue_dir<R, PT>(b, grp, d, grp.variant[d - 1])) return rc;
   return 0;
 }
 
@@ -413,6 +466,8 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   ph.srhd = c.metric_kind == GRHD2_METRIC_MINKOWSKI && c.geom_kind == GRHD2_GEOM_CARTESIAN;
   ph.adb = c.adb_idx; ph.g1 = c.g1; ph.rho_floor = c.rho_floor; ph.p_floor = c.p_floor; ph.v_max = c.v_max;
   G.nx = c.nx; G.ny = c.ny; G.nz = c.nz; G.ng = c.nghost; G.case_id = c.case_id;
+  G.div_nx = make_fastdiv((unsigned)c.nx); G.div_ny = make_fastdiv((unsigned)c.ny);
+  G.div_nx1 = make_fastdiv((unsigned)c.nx + 1); G.div_ny1 = make_fastdiv((unsigned)c.ny + 1);
   G.ncell = (long long)c.nx * c.ny * c.nz;
   G.pplane = (G.ncell + 31) / 32 * 32;
   G.nij = (long long)c.nx * c.ny;
@@ -1004,6 +1059,79 @@ int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *ste
   if (t) *t = c.t;
   if (steps) *steps = c.steps;
   if (active) *active = c.active;
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant) {
+  if (!b) return GRHD2_ERR_ARG;
+  if (variant != GRHD2_FLUX_AUTO && variant != GRHD2_FLUX_SPLIT && variant != GRHD2_FLUX_FUSED)
+    return bfail(b, GRHD2_ERR_ARG, "invalid flux variant %d", variant);
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  b->variant_request = variant;
+  return build_batch(b);
+}
+
+int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *chosen, int cap, int *n_out) {
+  if (!b || reps <= 0) return bfail(b, GRHD2_ERR_ARG, "invalid arguments to autotune");
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  b->variant_request = GRHD2_FLUX_AUTO;
+  if (int rc = build_batch(b)) return rc;
+  const int n = (int)b->m.size();
+  // tuning launches count reconstruction clamps and HLLC fallbacks: save and restore
+  std::vector<unsigned long long> saved((size_t)n * NCNT);
+  for (int g = 0; g < n; ++g)
+    BCUDA_TRY(b, cudaMemcpyAsync(&saved[(size_t)g * NCNT], b->m[g]->G.cnt, NCNT * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, b->stream));
+  BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  std::vector<GridDev> hg(n);
+  for (int g = 0; g < n; ++g) hg[g] = b->m[g]->G;
+  cudaEvent_t e0, e1;
+  BCUDA_TRY(b, cudaEventCreate(&e0));
+  BCUDA_TRY(b, cudaEventCreate(&e1));
+  int rc = 0, k = 0;
+  for (auto &grp : b->groups) {
+    for (int d = 1; d <= 3 && !rc; ++d) {
+      if (grp.nb[K_FLUX_X + d - 1] <= 0) continue;
+      float best = 0.0f;
+      int best_v = DEFAULT_VARIANT;
+      for (int v : {GRHD2_FLUX_SPLIT, GRHD2_FLUX_FUSED}) {
+        auto run = [&]() { return grp.mixed ? enqueue_dir<float, float>(b, grp, d, v) : enqueue_dir<double, double>(b, grp, d, v); };
+        if ((rc = run())) break;  // warm-up
+        cudaEventRecord(e0, b->stream);
+        for (int r = 0; r < reps && !rc; ++r) rc = run();
+        cudaEventRecord(e1, b->stream);
+        if (rc) break;
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) { rc = bfail(b, GRHD2_ERR_CUDA, "autotune: %s", cudaGetErrorString(e)); break; }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (v == GRHD2_FLUX_SPLIT || t < best) { best = t; best_v = v; }
+      }
+      if (rc) break;
+      grp.variant[d - 1] = best_v;
+      {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune[tune_key(grp, hg, d)] = best_v;
+      }
+      if (chosen && k < cap) chosen[k] = best_v;
+      ++k;
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int g = 0; g < n; ++g)
+    cudaMemcpyAsync(b->m[g]->G.cnt, &saved[(size_t)g * NCNT], NCNT * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                    b->stream);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (rc) return rc;
+  if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+  // the captured step used the previous variants
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  if (n_out) *n_out = k;
   return GRHD2_OK;
 }
 

@@ -108,8 +108,16 @@ __device__ __forceinline__ void c2p_count(unsigned long long *cnt, unsigned fl) 
 // up into u, the "u = up" of grhd2.f90:232).
 // ------------------------------------------------------------------------------------
 // Batched: block b works on grid map[b].grid, cells map[b].first + threadIdx.x.
+// Resident 128-thread blocks per SM the register allocation must allow.  The kernel waits
+// on dependent FP64 chains (con2prim) and scattered table loads, so more warps in flight
+// pay for a few spilled registers: measured on the 2.5D torus batch, 8 blocks (64
+// registers) is fastest for FP64 and 6 (80 registers) for the mixed policy.
+template <class PT>
+constexpr int cell_min_blocks() { return sizeof(PT) == sizeof(double) ? 8 : 6; }
+
 template <int MODE, class R, class PT>
-__global__ void __launch_bounds__(128) k_cell_update(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+__global__ void __launch_bounds__(128, cell_min_blocks<PT>())
+    k_cell_update(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   const long long c = (long long)bm.first + threadIdx.x;
@@ -130,9 +138,10 @@ __global__ void __launch_bounds__(128) k_cell_update(const GridDev *__restrict__
     dt = clock_dt(ck);
   }
   unsigned long long *cnt = G.cnt;
-  const int i0 = (int)(c % G.nx);
-  const long long r = c / G.nx;
-  const int j0 = (int)(r % G.ny), k0 = (int)(r / G.ny);
+  const unsigned r = fdiv((unsigned)c, G.div_nx);
+  const int i0 = (int)((unsigned)c - r * G.div_nx.d);
+  const unsigned kk = fdiv(r, G.div_ny);
+  const int j0 = (int)(r - kk * G.div_ny.d), k0 = (int)kk;
   const long long ij = i0 + (long long)G.nx * j0;
   double q[NEQ];
 #pragma unroll
@@ -189,8 +198,16 @@ __global__ void __launch_bounds__(128) k_cell_update(const GridDev *__restrict__
     cs[v] = nv;
   }
   const CellMetric cm = load_cell_metric(G, ij);
+  // mixed policy: seed the root finder with the Lorentz factor of the current primitives
+  double W_seed = 0.0;
+  if (sizeof(PT) == sizeof(float)) {
+    const double a = q[EQ_VX], b = q[EQ_VY], d = q[EQ_VZ];
+    const double vsq = cm.g11 * a * a + cm.g22 * b * b + cm.g33 * d * d +
+                       2.0 * (cm.g12 * a * b + cm.g13 * a * d + cm.g23 * b * d);
+    W_seed = vsq < 1.0 ? 1.0 / sqrt(1.0 - vsq) : 0.0;
+  }
   double pr[NEQ];
-  const unsigned fl = cons_to_prim(P, cm, cs, pr);
+  const unsigned fl = cons_to_prim(P, cm, cs, pr, W_seed);
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) {
     UP[v * G.pplane + c] = cs[v];

@@ -599,8 +599,48 @@ __device__ inline double root_safe_newton(double g1, double rho_floor, double D,
   return root_brent(g1, rho_floor, D, tau, Q2);
 }
 
-// cons_to_prim, equations.f90:94-205: cons modified in place (intent(inout)); returns flags
-__device__ inline unsigned cons_to_prim(const Phys &P, const CellMetric &m, double (&cs)[NEQ], double (&pr)[NEQ]) {
+// Mixed-policy root finder: the same residual and bracket [1, max(1e3, 2 W_guess)] as
+// root_safe_newton, but Newton starts from W_seed (the Lorentz factor of the cell's
+// current primitives, a few 1e-3 off the root after one stage) instead of the bracket
+// midpoint, so it converges in a few iterations instead of ~10 bisections plus Newton.
+// f(1) = -Q2 <= 0 analytically (V is finite at W = 1 since g1 > 1), so the lower end needs
+// no evaluation.  Not converged after 20 iterations, or no sign change at the upper end:
+// the reference iteration decides (same result class as the FP64 path).
+__device__ inline double root_seeded_newton(double g1, double rho_floor, double D, double tau, double Q2,
+                                            double W_seed, unsigned &flags) {
+  const double x_acc = 1.0e-10;
+  if (Q2 < 1.0e-14) return 1.0;  // root_safe_newton: |f(1)| = Q2 < 1e-14 returns W = 1
+  const double Wg = (sqrt(Q2) + D) / rmax(D, rho_floor);
+  const double x2 = rmax(1.0e3, Wg * 2.0);
+  double lo = 1.0, hi = x2;
+  double root = (W_seed > 1.0 && W_seed < x2) ? W_seed : 0.5 * (1.0 + x2);
+  double f, df;
+  bool hi_checked = false;
+  for (int it = 0; it < 20; ++it) {
+    residual(g1, root, D, tau, Q2, f, df);
+    if (!(f == f) || !(df == df)) break;
+    if (f < 0.0) lo = root; else { hi = root; hi_checked = true; }
+    double next = root - f / df;
+    if (fabs(next - root) < x_acc) return next;  // converged Newton step
+    if (!(next > lo && next < hi)) {             // outside the bracket: bisect
+      if (!hi_checked) {                         // confirm the upper end brackets the root first
+        double fh, dfh;
+        residual(g1, x2, D, tau, Q2, fh, dfh);
+        if (!(fh > 0.0)) break;
+        hi_checked = true;
+      }
+      next = 0.5 * (lo + hi);
+      if (fabs(next - root) < x_acc) return next;
+    }
+    root = next;
+  }
+  return root_safe_newton(g1, rho_floor, D, tau, Q2, flags);
+}
+
+// cons_to_prim, equations.f90:94-205: cons modified in place (intent(inout)); returns flags.
+// W_seed > 0 selects the seeded root finder of the mixed policy; the FP64 path passes 0.
+__device__ inline unsigned cons_to_prim(const Phys &P, const CellMetric &m, double (&cs)[NEQ], double (&pr)[NEQ],
+                                        double W_seed = 0.0) {
   unsigned flags = 0;
   const double lDf = P.rho_floor * m.sqg;
   const double lTf = P.p_floor * (P.g1 - 1.0) * m.sqg;
@@ -623,7 +663,8 @@ __device__ inline unsigned cons_to_prim(const Phys &P, const CellMetric &m, doub
     }
     const double D = cs[EQ_DE], tau = cs[EQ_PR];
     const double Q2 = qsq(m, cs[EQ_VX], cs[EQ_VY], cs[EQ_VZ]);
-    const double W = root_safe_newton(P.g1, P.rho_floor, D, tau, Q2, flags);
+    const double W = W_seed > 0.0 ? root_seeded_newton(P.g1, P.rho_floor, D, tau, Q2, W_seed, flags)
+                                  : root_safe_newton(P.g1, P.rho_floor, D, tau, Q2, flags);
     if (W < 1.0) {
       flags |= C2P_ROOT_FAIL;
       floor_state = true;

@@ -60,12 +60,29 @@ __host__ __device__ __forceinline__ double clock_dt(const GridClock &c) {
 }
 __host__ __device__ __forceinline__ bool clock_skip(const GridClock &c) { return c.mode == 1 && !c.active; }
 
+// Division by a grid extent with a multiply-high and a shift (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", 1994): for d >= 1 with
+// l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1, n / d = (umulhi(n, m) + n) >> l
+// for every n < 2^31 (the sum cannot overflow).  Face and cell counts per grid are below
+// 2^31 (checked at create), so the index decode needs no integer division instruction.
+struct FastDiv {
+  unsigned d, m, l;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+  unsigned l = 0;
+  while ((1ull << l) < d) ++l;
+  const unsigned long long m = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
+  return FastDiv{d, (unsigned)m, l};
+}
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) { return (__umulhi(n, f.m) + n) >> f.l; }
+
 // Everything a kernel needs about one grid.  The stage kernels read these descriptors from
 // a device array, one entry per grid of a batch (a single grid is a batch of one).
 struct GridDev {
   // sizes
   int nx, ny, nz, ng;
   int case_id;
+  FastDiv div_nx, div_ny, div_nx1, div_ny1;  // nx, ny, nx + 1, ny + 1
   long long ncell;   // nx*ny*nz
   long long pplane;  // plane stride of the primitive / conserved arrays (elements)
   // metric tables
@@ -98,14 +115,18 @@ struct BlockMap {
 };
 
 // interior primitive read (1-based cell indices)
+// (cell counts are below 2^31, so the linear cell index is computed in 32 bits)
+__device__ __forceinline__ unsigned cell_index(const GridDev &G, int i, int j, int k) {
+  return (unsigned)(i - 1) + (unsigned)G.nx * ((unsigned)(j - 1) + (unsigned)G.ny * (unsigned)(k - 1));
+}
 template <class PT>
 __device__ __forceinline__ double ld_prim(const PT *__restrict__ P, const GridDev &G, int v, int i, int j, int k) {
-  const long long c = (long long)(i - 1) + (long long)G.nx * ((long long)(j - 1) + (long long)G.ny * (k - 1));
+  const unsigned c = cell_index(G, i, j, k);
   return (double)__ldg(&P[v * G.pplane + c]);
 }
 template <class PT>
 __device__ __forceinline__ void ld_cell(const PT *__restrict__ P, const GridDev &G, int i, int j, int k, double (&q)[NEQ]) {
-  const long long c = (long long)(i - 1) + (long long)G.nx * ((long long)(j - 1) + (long long)G.ny * (k - 1));
+  const unsigned c = cell_index(G, i, j, k);
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) q[v] = (double)__ldg(&P[v * G.pplane + c]);
 }

@@ -75,6 +75,8 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--batch", type=int, default=1, help="replicas stepped as one batch")
     ap.add_argument("--graph", type=int, default=1, help="replay each step as a CUDA graph")
+    ap.add_argument("--flux", choices=["auto", "split", "fused", "tune"], default="tune",
+                    help="face-flux kernel variant ('tune': time both on this batch)")
     args, rest = ap.parse_known_args(argv)
     overrides = _parse_overrides(rest)
     from .problem import Problem
@@ -109,6 +111,7 @@ def main(argv=None):
     batch = GpuBatch(grids)
     for k in range(len(grids)):
         batch.set_clock(k, 0.0, 1e300, -1)
+    tuned = batch.autotune() if args.flux == "tune" else batch.set_flux_variant(args.flux)
     batch.step(args.warmup, graph=args.graph)
     g.synchronize()
     t0 = time.perf_counter()
@@ -119,7 +122,7 @@ def main(argv=None):
     cells = pb.n_cells * len(grids)
     out = {"cells": cells, "grids": len(grids), "steps": args.steps, "dt": g.cfl(),
            "ms_per_step": el / args.steps * 1e3, "zone_updates_per_s": cells * args.steps / el,
-           "kernels": prof, "counters": g.counters()}
+           "kernels": prof, "counters": g.counters(), "flux_variant": tuned or args.flux}
     batch.close()
     for gr in reversed(grids):
         gr.close()

@@ -250,6 +250,22 @@ class GpuBatch:
         self._check(self.lib.grhd2_gpu_batch_get_clock(self._b, k, C.byref(t), C.byref(n), C.byref(a)))
         return t.value, n.value, bool(a.value)
 
+    FLUX_VARIANTS = {"auto": -1, "split": 0, "fused": 1}
+
+    def set_flux_variant(self, variant: str):
+        """'split' (recon + Riemann kernels), 'fused' (one kernel) or 'auto' (tuned/cached)."""
+        self._check(self.lib.grhd2_gpu_batch_set_flux_variant(self._b, self.FLUX_VARIANTS[variant]))
+
+    def autotune(self, reps: int = 5):
+        """Time both flux variants per scheme group and direction; returns the choices
+        (group order, x before y before z) as variant names."""
+        cap = 64
+        out = (C.c_int * cap)()
+        n = C.c_int()
+        self._check(self.lib.grhd2_gpu_batch_autotune(self._b, reps, out, cap, C.byref(n)))
+        names = {v: k for k, v in self.FLUX_VARIANTS.items()}
+        return [names[out[k]] for k in range(min(n.value, cap))]
+
     def profile_step(self):
         """[(kernel name, ms)] for every launch of one batched step."""
         cap = 256

@@ -192,6 +192,19 @@ int grhd2_gpu_batch_step(grhd2_gpu_batch *b, int nsteps, int use_graph);
 int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *steps, int *active);
 /* Per-launch timing of one batched step (names/ms as in grhd2_gpu_profile_step). */
 int grhd2_gpu_batch_profile_step(grhd2_gpu_batch *b, float *ms, const char **names, int cap, int *n_out);
+/* Kernel variants of the face fluxes of one direction. */
+#define GRHD2_FLUX_AUTO -1  /* the autotuned choice for this shape if one is cached, else SPLIT */
+#define GRHD2_FLUX_SPLIT 0  /* reconstruction kernel (thread per face and variable) + Riemann kernel */
+#define GRHD2_FLUX_FUSED 1  /* one kernel, thread per face, interface states kept on chip */
+/* Use one variant for every scheme group and direction of the batch (or AUTO). */
+int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant);
+/* Time each variant (reps launches after a warm-up) per scheme group and active direction
+ * on the batch's current state and keep the faster one; the choice is also cached for
+ * later batches of the same precision, scheme, solver, sensor, direction and size class.
+ * The state and counters are left unchanged.  chosen[k] (k < cap) receives the variants in
+ * group order, x before y before z; *n_out their number.  Call after the state is set (a
+ * grid whose clock is finished does no work and cannot be timed). */
+int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *chosen, int cap, int *n_out);
 const char *grhd2_gpu_batch_last_error(const grhd2_gpu_batch *b);
 void grhd2_gpu_batch_destroy(grhd2_gpu_batch *b);
 /* The handle's CUDA stream (a cudaStream_t) so callers can order their own work and

@@ -40,12 +40,13 @@ def _make(pb, stream, precision="fp64"):
     return g, p0
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_batch_matches_oracle_per_grid(graph):
+@pytest.mark.parametrize("graph,variant", [(True, "split"), (False, "split"), (True, "fused"), (False, "fused")])
+def test_batch_matches_oracle_per_grid(graph, variant):
     s = _stream()
     cases = _cases()
     grids, p0s = zip(*[_make(pb, s) for pb, _, _ in cases])
     b = GpuBatch(list(grids))
+    b.set_flux_variant(variant)
     for k, (pb, tf, ms) in enumerate(cases):
         b.set_clock(k, 0.0, tf, ms)
     # enough replays for the longest grid; finished grids idle
@@ -103,11 +104,45 @@ def test_batch_profile_names():
     s = _stream()
     grids = [_make(pb, s)[0] for pb in (torus_3d(nx=16, ny=8, nz=8), shock_tube(nx=64))]
     b = GpuBatch(grids)
+    b.set_flux_variant("split")
     for k in range(2):
         b.set_clock(k, 0.0, 1e30, 1)
     names = [n for n, _ in b.profile_step()]
     assert names.count("cell_update") == 3 * 2  # two scheme groups, three stages
     assert "recon_z" in names and "riemann_y" in names and names[-1] == "advance_clocks"
+    b.set_flux_variant("fused")
+    names = [n for n, _ in b.profile_step()]
+    assert names.count("flux_x") == 3 * 2 and names.count("flux_z") == 3 and "recon_x" not in names
+    b.close()
+    for g in grids:
+        g.close()
+
+
+def test_autotune_leaves_state_and_counters():
+    """Autotuning times both flux variants on the live state: afterwards the state and the
+    counters are unchanged, and stepping with the tuned variants gives the solo result."""
+    s = _stream()
+    pbs = [torus_3d(nx=24, ny=12, nz=12), shock_tube(nx=200, rec="weno5", rs="hlle", sensor=True)]
+    solo = []
+    for pb in pbs:
+        g, _ = _make(pb, s)
+        g.run(0.0, 1e30, 4)
+        solo.append((g.download(want_p=False)[0], g.counters()))
+        g.close()
+    grids = [_make(pb, s)[0] for pb in pbs]
+    b = GpuBatch(grids)
+    for k in range(len(grids)):
+        b.set_clock(k, 0.0, 1e30, 4)
+    before = [(g.download(want_p=False)[0], g.counters()) for g in grids]
+    chosen = b.autotune(reps=2)
+    assert len(chosen) == 3 + 1 and set(chosen) <= {"split", "fused"}
+    for g, (up, cnt) in zip(grids, before):
+        up2 = g.download(want_p=False)[0]
+        assert np.array_equal(up, up2) and g.counters() == cnt
+    b.step(6, graph=True)
+    for k, g in enumerate(grids):
+        assert np.array_equal(g.download(want_p=False)[0], solo[k][0])
+        assert g.counters() == solo[k][1]
     b.close()
     for g in grids:
         g.close()
