@@ -335,6 +335,8 @@ def run_ours(args):
                               "frac": STEP_BYTES_PER_ZONE["fp64"] * value / world / 1e9 / peak,
                               "mixed_achieved": STEP_BYTES_PER_ZONE["mixed"] * mixed_value / world / 1e9}},
     }
+    if args.serve_requests > 0:
+        out["serve"] = run_serve(args)
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(pb, initial_state(pb), max_seconds=args.cpu_seconds)
     if world > 1:
@@ -342,6 +344,23 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def run_serve(args):
+    """A bounded sample of the serving stream (Poisson arrivals, 70 % Riemann problems of
+    128-8192 cells to t = 0.4, 30 % Michel runs of 512-4096 cells) through the
+    continuous-batching server on this GPU: time to solution p50/p99 and zone-updates/s."""
+    from grhd_b200.serve import GpuEngine, SolveServer, make_stream, summarize
+    reqs = make_stream(args.serve_requests, seed=20260901, rate=args.serve_rate,
+                       michel_final_time=args.serve_michel_final_time)
+    srv = SolveServer(GpuEngine("fp64"), steps_per_round=16)
+    res = srv.run(reqs)
+    out = summarize(res)
+    out.update(peak_active=srv.peak_active, rounds=srv.rounds, batch_rebuilds=srv.rebuilds,
+               sample=f"{args.serve_requests} requests of the 4096-request stream (seed 20260901), "
+                      f"{args.serve_rate:g} arrivals/s, Michel final time {args.serve_michel_final_time:g} M, FP64",
+               timing="wall clock from each arrival to its result on the host")
+    return out
 
 
 def cpu_baseline(pb, p0, max_seconds=15.0, steps=None):
@@ -390,6 +409,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--batch", type=int, default=32, help="torus grids per GPU stepped as one batch")
+    ap.add_argument("--serve-requests", type=int, default=256, help="serving sample size (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-michel-final-time", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

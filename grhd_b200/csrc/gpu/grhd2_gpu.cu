@@ -107,6 +107,7 @@ struct grhd2_gpu_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
   GridDev *d_grids = nullptr;
+  GridClock *d_clocks = nullptr;  // gathered clocks of every member (grhd2_gpu_batch_clocks)
   std::vector<Group> groups;
   int variant_request = GRHD2_FLUX_AUTO;  // GRHD2_FLUX_AUTO: tuned choice if cached, else the default
   cudaGraph_t graph = nullptr;
@@ -182,6 +183,8 @@ void destroy_batch_resources(grhd2_gpu_batch *b) {
   b->groups.clear();
   if (b->d_grids) cudaFree(b->d_grids);
   b->d_grids = nullptr;
+  if (b->d_clocks) cudaFree(b->d_clocks);
+  b->d_clocks = nullptr;
 }
 
 // ---- flux variant choice --------------------------------------------------------------
@@ -224,6 +227,7 @@ int build_batch(grhd2_gpu_batch *b) {
   b->versions.resize(n);
   for (int g = 0; g < n; ++g) { hg[g] = b->m[g]->G; b->versions[g] = b->m[g]->version; }
   BCUDA_TRY(b, cudaMalloc((void **)&b->d_grids, sizeof(GridDev) * n));
+  BCUDA_TRY(b, cudaMalloc((void **)&b->d_clocks, sizeof(GridClock) * n));
   BCUDA_TRY(b, cudaMemcpyAsync(b->d_grids, hg.data(), sizeof(GridDev) * n, cudaMemcpyHostToDevice, b->stream));
   for (int g = 0; g < n; ++g) {
     const grhd2_gpu *h = b->m[g];
@@ -318,6 +322,9 @@ int enqueue_step(grhd2_gpu_batch *b) {
 }
 
 int batch_steps(grhd2_gpu_batch *b, long long nsteps, bool use_graph) {
+  for (size_t g = 0; g < b->m.size(); ++g)
+    if (b->m[g]->stream != b->stream)
+      return bfail(b, GRHD2_ERR_STATE, "grid %zu moved to another stream after the batch was created", g);
   if (int rc = refresh_batch(b)) return rc;
   if (nsteps <= 0) return 0;
   if (!use_graph) {
@@ -425,8 +432,78 @@ int profile_common(grhd2_gpu_batch *b, float *ms, const char **names, int cap, i
 
 }  // namespace
 
+// device bytes a handle of this configuration allocates (create + set_metric + set_bc_data;
+// the calc_rhs scratch is not counted), each allocation rounded up to 4 KB
+long long handle_bytes(const grhd2_gpu_config &c) {
+  const long long es = c.precision_policy == GRHD2_PREC_MIXED ? 4 : 8;
+  const long long ncell = (long long)c.nx * c.ny * c.nz, pplane = (ncell + 31) / 32 * 32;
+  const long long nf[3] = {(long long)(c.nx + 1) * c.ny * c.nz, (long long)c.nx * (c.ny + 1) * c.nz,
+                           (long long)c.nx * c.ny * (c.nz + 1)};
+  std::vector<long long> a;
+  a.push_back(5 * pplane * es);
+  a.push_back(5 * pplane * 8);
+  a.push_back(5 * pplane * 8);
+  long long nq = nf[0];
+  for (int d = 0; d < 3; ++d) {
+    if ((d == 1 && c.ny == 1) || (d == 2 && c.nz == 1)) continue;
+    nq = std::max(nq, nf[d]);
+    a.push_back(5 * nf[d] * es);
+  }
+  a.push_back(10 * nq * es);
+  a.push_back(NCNT * 8);
+  a.push_back((long long)sizeof(GridClock));
+  a.push_back(32);
+  a.push_back(5LL * (c.nx + 2 * c.nghost + 1) * (c.ny + 2 * c.nghost + 1) * (c.nz + 2 * c.nghost + 1) * 8);
+  if (c.nghost == 2) {
+    a.push_back(5LL * c.ny * c.nz * 8);
+    a.push_back(5LL * c.nx * c.nz * 8);
+    a.push_back(5LL * c.nx * c.ny * 8);
+  }
+  a.push_back((long long)NCF * c.nx * c.ny * 8);
+  a.push_back((long long)NFF * (c.nx + 1) * c.ny * 8);
+  if (c.ny > 1) a.push_back((long long)NFF * c.nx * (c.ny + 1) * 8);
+  if (c.nz > 1) a.push_back((long long)NFF * c.nx * c.ny * 8);
+  if (c.case_id == 7) a.push_back(5LL * c.nghost * c.ny * c.nz * 8);
+  if (c.case_id == 8) a.push_back(5LL * c.nghost * 8);
+  if (c.case_id == 5) a.push_back((long long)(c.nx + 2 * c.nghost + 1) * 8);
+  long long tot = 0;
+  for (long long x : a) tot += (std::max(x, 1LL) + 4095) / 4096 * 4096;
+  return tot;
+}
+
+__global__ void k_gather_clocks(const GridDev *__restrict__ grids, int n, GridClock *__restrict__ out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < n) out[g] = *grids[g].clock;
+}
+
 // ======================================================================================
 extern "C" {
+
+int64_t grhd2_gpu_device_bytes(const grhd2_gpu_config *cfg) {
+  if (!cfg || cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1 || cfg->nghost < 1) return -1;
+  return handle_bytes(*cfg);
+}
+
+int grhd2_gpu_set_stream(grhd2_gpu *h, void *stream) {
+  if (!h) return GRHD2_ERR_ARG;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (h->own_stream) CUDA_TRY(h, cudaStreamDestroy(h->stream));
+  h->own_stream = false;
+  h->stream = nullptr;
+  if (stream) {
+    h->stream = (cudaStream_t)stream;
+  } else {
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  if (h->self) {  // the batch of one follows the handle; its graph was captured for the old stream
+    destroy_batch_resources(h->self);
+    delete h->self;
+    h->self = nullptr;
+  }
+  return GRHD2_OK;
+}
 
 int grhd2_gpu_abi_version(void) { return GRHD2_GPU_ABI_VERSION; }
 
@@ -1059,6 +1136,24 @@ int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *ste
   if (t) *t = c.t;
   if (steps) *steps = c.steps;
   if (active) *active = c.active;
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *active) {
+  if (!b) return GRHD2_ERR_ARG;
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  if (int rc = refresh_batch(b)) return rc;
+  const int n = (int)b->m.size();
+  std::vector<GridClock> c(n);
+  k_gather_clocks<<<nblocks(n, 128), 128, 0, b->stream>>>(b->d_grids, n, b->d_clocks);
+  if (int rc = blaunch_check(b, "gather_clocks")) return rc;
+  BCUDA_TRY(b, cudaMemcpyAsync(c.data(), b->d_clocks, sizeof(GridClock) * n, cudaMemcpyDeviceToHost, b->stream));
+  BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  for (int g = 0; g < n; ++g) {
+    if (t) t[g] = c[g].t;
+    if (steps) steps[g] = c[g].steps;
+    if (active) active[g] = c[g].active;
+  }
   return GRHD2_OK;
 }
 

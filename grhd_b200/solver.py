@@ -140,6 +140,15 @@ class GpuGrid:
     def synchronize(self):
         self._check(self.lib.grhd2_gpu_synchronize(self._h))
 
+    def set_stream(self, stream: int | None):
+        """Move the handle to another cudaStream_t (None: a new private stream)."""
+        self._check(self.lib.grhd2_gpu_set_stream(self._h, C.c_void_p(stream) if stream else None))
+
+    @property
+    def device_bytes(self) -> int:
+        """Device bytes the handle allocated (the admission estimate of its config)."""
+        return int(self.lib.grhd2_gpu_device_bytes(C.byref(self.cfg)))
+
     @property
     def stream_ptr(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
@@ -243,6 +252,16 @@ class GpuBatch:
     def step(self, nsteps: int = 1, graph: bool = True):
         """Enqueue nsteps batched steps (asynchronous)."""
         self._check(self.lib.grhd2_gpu_batch_step(self._b, nsteps, 1 if graph else 0))
+
+    def clocks(self):
+        """(t, steps, active) arrays of every grid in one device read (synchronises)."""
+        n = len(self.grids)
+        t = np.empty(n)
+        st = np.empty(n, dtype=np.int64)
+        ac = np.empty(n, dtype=np.int32)
+        self._check(self.lib.grhd2_gpu_batch_clocks(
+            self._b, N.dptr(t), st.ctypes.data_as(C.POINTER(C.c_int64)), ac.ctypes.data_as(C.POINTER(C.c_int))))
+        return t, st, ac.astype(bool)
 
     def clock(self, k: int):
         """(t, steps, active) of grid k (synchronises the stream)."""

@@ -180,6 +180,14 @@ typedef struct grhd2_gpu_batch grhd2_gpu_batch;
 /* Like grhd2_gpu_create, but the handle works on the caller's CUDA stream (a cudaStream_t;
  * NULL creates a private stream).  Handles that will be batched must share one stream. */
 int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_gpu **out);
+/* Move a handle to another stream (NULL: a new private stream) after finishing its work
+ * on the old one.  Lets a caller prepare a grid on its own stream, overlapping work that
+ * runs on the batch stream, and then join it to a batch.  A batch that holds the handle
+ * refuses to step until it is recreated. */
+int grhd2_gpu_set_stream(grhd2_gpu *h, void *stream);
+/* Device bytes a handle of this configuration allocates (for admission by free memory);
+ * -1 for an invalid configuration. */
+int64_t grhd2_gpu_device_bytes(const grhd2_gpu_config *cfg);
 /* Group n handles (same device and stream, metric and state uploaded). */
 int grhd2_gpu_batch_create(grhd2_gpu **handles, int n, grhd2_gpu_batch **out);
 /* Set grid k's clock: time t0, final time, and a step limit (< 0: none).  The CFL dt is
@@ -192,6 +200,9 @@ int grhd2_gpu_batch_step(grhd2_gpu_batch *b, int nsteps, int use_graph);
 int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *steps, int *active);
 /* Per-launch timing of one batched step (names/ms as in grhd2_gpu_profile_step). */
 int grhd2_gpu_batch_profile_step(grhd2_gpu_batch *b, float *ms, const char **names, int cap, int *n_out);
+/* Clocks of every member in one call (arrays of n entries, any may be NULL); synchronises
+ * the batch stream. */
+int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *active);
 /* Kernel variants of the face fluxes of one direction. */
 #define GRHD2_FLUX_AUTO -1  /* the autotuned choice for this shape if one is cached, else SPLIT */
 #define GRHD2_FLUX_SPLIT 0  /* reconstruction kernel (thread per face and variable) + Riemann kernel */
