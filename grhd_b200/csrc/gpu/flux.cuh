@@ -24,28 +24,27 @@ struct FaceIndex {
   long long ft;       // face-table index (k-invariant)
 };
 
+// extents of the face index space of direction DIR (faces along DIR: n + 1)
 template <int DIR>
-__device__ __forceinline__ FaceIndex decode_face(const GridDev &G, long long f64) {
+__device__ __forceinline__ void face_space(const GridDev &G, unsigned &nI, unsigned &nJ, unsigned &nK) {
+  nI = (unsigned)G.nx + (DIR == 1 ? 1u : 0u);
+  nJ = (unsigned)G.ny + (DIR == 2 ? 1u : 0u);
+  nK = (unsigned)G.nz + (DIR == 3 ? 1u : 0u);
+}
+
+// face (a, b, c) of the index space: strip cell indices, face number along DIR, table index
+template <int DIR>
+__device__ __forceinline__ FaceIndex face_at(const GridDev &G, unsigned a, unsigned b, unsigned c) {
   FaceIndex x;
-  const unsigned f = (unsigned)f64;  // < 2^31 faces per grid
   if (DIR == 1) {
-    const unsigned r = fdiv(f, G.div_nx1);
-    x.face = (int)(f - r * G.div_nx1.d);
-    const unsigned k = fdiv(r, G.div_ny);
-    x.j = (int)(r - k * G.div_ny.d) + 1; x.k = (int)k + 1; x.i = x.face;
-    x.ft = x.face + (long long)(G.nx + 1) * (x.j - 1);
+    x.face = (int)a; x.i = (int)a; x.j = (int)b + 1; x.k = (int)c + 1;
+    x.ft = (long long)a + (long long)(G.nx + 1) * b;
   } else if (DIR == 2) {
-    const unsigned r = fdiv(f, G.div_nx);
-    x.i = (int)(f - r * G.div_nx.d) + 1;
-    const unsigned k = fdiv(r, G.div_ny1);
-    x.face = (int)(r - k * G.div_ny1.d); x.k = (int)k + 1; x.j = x.face;
-    x.ft = (x.i - 1) + (long long)G.nx * x.face;
+    x.i = (int)a + 1; x.face = (int)b; x.j = (int)b; x.k = (int)c + 1;
+    x.ft = (long long)a + (long long)G.nx * b;
   } else {
-    const unsigned r = fdiv(f, G.div_nx);
-    x.i = (int)(f - r * G.div_nx.d) + 1;
-    const unsigned k = fdiv(r, G.div_ny);
-    x.j = (int)(r - k * G.div_ny.d) + 1; x.face = (int)k; x.k = x.face;
-    x.ft = (x.i - 1) + (long long)G.nx * (x.j - 1);
+    x.i = (int)a + 1; x.j = (int)b + 1; x.face = (int)c; x.k = (int)c;
+    x.ft = (long long)a + (long long)G.nx * b;
   }
   return x;
 }
@@ -137,7 +136,7 @@ __device__ __forceinline__ void recon_one(int br, int lim, const R (&s)[6], R &q
   if (REC == REC_WENO5) { qL = weno5(s[0], s[1], s[2], s[3], s[4]); qR = weno5(s[5], s[4], s[3], s[2], s[1]); return; }
 }
 
-// Batched launches: block b works on grid map[b].grid, faces map[b].first + threadIdx.x.
+// Batched launches: block b works on grid map[b].grid, tile map[b].first / blockDim.x.
 // Q layout per grid: Q[(side*5 + v) * nfaces + f], side 0 = q_L, 1 = q_R
 // Resident blocks per SM the register allocation must allow (256-thread recon blocks,
 // 128-thread Riemann blocks).  Both kernels stall on dependent FP64 chains, so occupancy
@@ -155,13 +154,17 @@ __global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const Grid
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;
   const long long nf = n_faces<DIR>(G);
-  const long long f = (long long)bm.first + threadIdx.x;
   const int v = blockIdx.y;
-  if (f >= nf || clock_skip(*G.clock)) return;
+  unsigned nI, nJ, nK, a, b, c;
+  face_space<DIR>(G, nI, nJ, nK);
+  if (!tile_item<8>(G.tiles[TILE_RECON + DIR - 1], (unsigned)bm.first >> 8, threadIdx.x, nI, nJ, nK, a, b, c) ||
+      clock_skip(*G.clock))
+    return;
+  const long long f = (long long)a + (long long)nI * ((long long)b + (long long)nJ * c);
   const PT *__restrict__ Pin = (const PT *)G.P;
   R *__restrict__ Q = (R *)G.Q;
   unsigned long long *cnt = G.cnt;
-  const FaceIndex x = decode_face<DIR>(G, f);
+  const FaceIndex x = face_at<DIR>(G, a, b, c);
   const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
   int lo, hi;
   stencil_range(REC, P.sensor, lo, hi);
@@ -225,10 +228,14 @@ __global__ void __launch_bounds__(FLUX_BS) k_flux(const GridDev *__restrict__ gr
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;
   const long long nf = n_faces<DIR>(G);
-  const long long f = (long long)bm.first + threadIdx.x;
-  if (f >= nf || clock_skip(*G.clock)) return;
+  unsigned nI, nJ, nK, a, b, c;
+  face_space<DIR>(G, nI, nJ, nK);
+  if (!tile_item<7>(G.tiles[TILE_FACE + DIR - 1], (unsigned)bm.first >> 7, threadIdx.x, nI, nJ, nK, a, b, c) ||
+      clock_skip(*G.clock))
+    return;
+  const long long f = (long long)a + (long long)nI * ((long long)b + (long long)nJ * c);
   const PT *__restrict__ Pin = (const PT *)G.P;
-  const FaceIndex x = decode_face<DIR>(G, f);
+  const FaceIndex x = face_at<DIR>(G, a, b, c);
   const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
   int lo, hi;
   stencil_range(REC, P.sensor, lo, hi);
@@ -303,12 +310,16 @@ __global__ void __launch_bounds__(128, GRHD_RIEMANN_MIN_BLOCKS) k_riemann(const 
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;
   const long long nf = n_faces<DIR>(G);
-  const long long f = (long long)bm.first + threadIdx.x;
-  if (f >= nf || clock_skip(*G.clock)) return;
+  unsigned nI, nJ, nK, a, b, c;
+  face_space<DIR>(G, nI, nJ, nK);
+  if (!tile_item<7>(G.tiles[TILE_FACE + DIR - 1], (unsigned)bm.first >> 7, threadIdx.x, nI, nJ, nK, a, b, c) ||
+      clock_skip(*G.clock))
+    return;
+  const long long f = (long long)a + (long long)nI * ((long long)b + (long long)nJ * c);
   const R *__restrict__ Q = (const R *)G.Q;
   R *__restrict__ F = (R *)G.F[DIR - 1];
   unsigned long long *cnt = G.cnt;
-  const FaceIndex x = decode_face<DIR>(G, f);
+  const FaceIndex x = face_at<DIR>(G, a, b, c);
   R qL[NEQ], qR[NEQ], flux[NEQ];
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) { qL[v] = Q[(long long)v * nf + f]; qR[v] = Q[(long long)(5 + v) * nf + f]; }

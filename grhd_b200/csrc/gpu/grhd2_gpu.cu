@@ -54,14 +54,62 @@ const int KIND_BS[NKIND] = {RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, RECON_BS
 const char *KIND_NAME[NKIND] = {"recon_x", "riemann_x", "recon_y", "riemann_y", "recon_z", "riemann_z",
                                 "cell_update", "flux_x", "flux_y", "flux_z"};
 
+// ---- block tiles ------------------------------------------------------------------------
+unsigned ilog2(unsigned x) {
+  unsigned l = 0;
+  while ((1u << (l + 1)) <= x) ++l;
+  return l;
+}
+// extents of the index space of a tile kind (cells, or faces of direction dir)
+void space_of(const GridDev &G, int dir, unsigned &nI, unsigned &nJ, unsigned &nK) {
+  nI = (unsigned)G.nx + (dir == 1); nJ = (unsigned)G.ny + (dir == 2); nK = (unsigned)G.nz + (dir == 3);
+}
+// tile of 2^lb threads: tx along i (the whole block for 1D grids), the rest along k, or
+// along j when the grid has no k extent
+Tile make_tile(unsigned nI, unsigned nJ, unsigned nK, unsigned lb, unsigned tx) {
+  Tile T;
+  T.lx = std::min(ilog2(std::max(tx, 1u)), lb);
+  if (nJ == 1 && nK == 1) T.lx = lb;
+  T.ly = nK == 1 ? lb - T.lx : 0;
+  T.nti = make_fastdiv((nI + (1u << T.lx) - 1) >> T.lx);
+  T.ntj = make_fastdiv((nJ + (1u << T.ly) - 1) >> T.ly);
+  return T;
+}
+long long tile_count(const Tile &T, unsigned lb, unsigned nK) {
+  const unsigned lz = lb - T.lx - T.ly;
+  return (long long)T.nti.d * T.ntj.d * ((nK + (1u << lz) - 1) >> lz);
+}
+constexpr unsigned LB_RECON = 8, LB_FACE = 7, LB_CELL = 7;  // log2 of RECON_BS, RIEMANN_BS = FUSED_FLUX_BS, CELL_BS
+static_assert((1 << LB_RECON) == RECON_BS && (1 << LB_FACE) == RIEMANN_BS && (1 << LB_FACE) == FUSED_FLUX_BS &&
+                  (1 << LB_CELL) == CELL_BS, "block sizes are the tile sizes");
+constexpr unsigned DEFAULT_TX = 32;
+
+void set_face_tiles(GridDev &G, int dir, unsigned tx) {
+  unsigned nI, nJ, nK;
+  space_of(G, dir, nI, nJ, nK);
+  G.tiles[TILE_RECON + dir - 1] = make_tile(nI, nJ, nK, LB_RECON, tx);
+  G.tiles[TILE_FACE + dir - 1] = make_tile(nI, nJ, nK, LB_FACE, tx);
+}
+void set_cell_tile(GridDev &G, unsigned tx) {
+  G.tiles[TILE_CELL] = make_tile((unsigned)G.nx, (unsigned)G.ny, (unsigned)G.nz, LB_CELL, tx);
+}
+
+bool dir_active(const GridDev &G, int dir) { return !((dir == 2 && G.ny == 1) || (dir == 3 && G.nz == 1)); }
+long long face_count(const GridDev &G, int dir) {
+  unsigned nI, nJ, nK;
+  space_of(G, dir, nI, nJ, nK);
+  return (long long)nI * nJ * nK;
+}
+
+// threads (tiles x block size) a kernel kind launches for one grid
 long long kind_items(const GridDev &G, int k) {
-  if (k == K_CELL) return G.ncell;
+  if (k == K_CELL) return tile_count(G.tiles[TILE_CELL], LB_CELL, (unsigned)G.nz) * CELL_BS;
   const int dir = k >= K_FLUX_X ? k - K_FLUX_X + 1 : k / 2 + 1;
-  if (dir == 2 && G.ny == 1) return 0;
-  if (dir == 3 && G.nz == 1) return 0;
-  if (dir == 1) return (long long)(G.nx + 1) * G.ny * G.nz;
-  if (dir == 2) return (long long)G.nx * (G.ny + 1) * G.nz;
-  return (long long)G.nx * G.ny * (G.nz + 1);
+  if (!dir_active(G, dir)) return 0;
+  unsigned nI, nJ, nK;
+  space_of(G, dir, nI, nJ, nK);
+  if (k < K_CELL && (k % 2) == 0) return tile_count(G.tiles[TILE_RECON + dir - 1], LB_RECON, nK) * RECON_BS;
+  return tile_count(G.tiles[TILE_FACE + dir - 1], LB_FACE, nK) * RIEMANN_BS;
 }
 
 inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -99,6 +147,12 @@ struct Group {
   BlockMap *d_map = nullptr;
   int off[NKIND], nb[NKIND];
   int variant[3];  // per direction: GRHD2_FLUX_SPLIT or GRHD2_FLUX_FUSED
+  unsigned tx[3];  // per direction: tile extent along i of the face kernels
+};
+
+struct FluxChoice {
+  int variant;
+  unsigned tx;
 };
 
 struct grhd2_gpu_batch {
@@ -110,6 +164,8 @@ struct grhd2_gpu_batch {
   GridClock *d_clocks = nullptr;  // gathered clocks of every member (grhd2_gpu_batch_clocks)
   std::vector<Group> groups;
   int variant_request = GRHD2_FLUX_AUTO;  // GRHD2_FLUX_AUTO: tuned choice if cached, else the default
+  unsigned tile_request = 0;              // 0: tuned tile if cached, else DEFAULT_TX
+  std::map<std::pair<int, int>, FluxChoice> forced;  // (group, direction) -> choice, while tuning
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool profiling = false;
@@ -199,11 +255,11 @@ struct TuneKey {
   }
 };
 std::mutex g_tune_mu;
-std::map<TuneKey, int> g_tune;
+std::map<TuneKey, FluxChoice> g_tune;
 
 TuneKey tune_key(const Group &grp, const std::vector<GridDev> &hg, int dir) {
   long long faces = 0;
-  for (int g : grp.members) faces += kind_items(hg[g], 2 * (dir - 1));
+  for (int g : grp.members) faces += face_count(hg[g], dir);
   int cls = 0;
   while ((1LL << (cls + 1)) <= faces) ++cls;
   return TuneKey{grp.mixed ? 1 : 0, grp.rec, grp.rs, hg[grp.members[0]].phys.sensor, dir, cls};
@@ -212,11 +268,18 @@ TuneKey tune_key(const Group &grp, const std::vector<GridDev> &hg, int dir) {
 // default without tuning: the split kernels (recon at high occupancy, lean Riemann)
 constexpr int DEFAULT_VARIANT = GRHD2_FLUX_SPLIT;
 
-int choose_variant(const grhd2_gpu_batch *b, const Group &grp, const std::vector<GridDev> &hg, int dir) {
-  if (b->variant_request == GRHD2_FLUX_SPLIT || b->variant_request == GRHD2_FLUX_FUSED) return b->variant_request;
-  std::lock_guard<std::mutex> lock(g_tune_mu);
-  auto it = g_tune.find(tune_key(grp, hg, dir));
-  return it == g_tune.end() ? DEFAULT_VARIANT : it->second;
+FluxChoice choose_flux(const grhd2_gpu_batch *b, int gi, const Group &grp, const std::vector<GridDev> &hg, int dir) {
+  auto f = b->forced.find({gi, dir});
+  if (f != b->forced.end()) return f->second;
+  FluxChoice c{DEFAULT_VARIANT, DEFAULT_TX};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(tune_key(grp, hg, dir));
+    if (it != g_tune.end()) c = it->second;
+  }
+  if (b->variant_request == GRHD2_FLUX_SPLIT || b->variant_request == GRHD2_FLUX_FUSED) c.variant = b->variant_request;
+  if (b->tile_request > 0) c.tx = b->tile_request;
+  return c;
 }
 
 // (re)build device descriptors and block maps of a batch
@@ -226,20 +289,32 @@ int build_batch(grhd2_gpu_batch *b) {
   std::vector<GridDev> hg(n);
   b->versions.resize(n);
   for (int g = 0; g < n; ++g) { hg[g] = b->m[g]->G; b->versions[g] = b->m[g]->version; }
-  BCUDA_TRY(b, cudaMalloc((void **)&b->d_grids, sizeof(GridDev) * n));
-  BCUDA_TRY(b, cudaMalloc((void **)&b->d_clocks, sizeof(GridClock) * n));
-  BCUDA_TRY(b, cudaMemcpyAsync(b->d_grids, hg.data(), sizeof(GridDev) * n, cudaMemcpyHostToDevice, b->stream));
   for (int g = 0; g < n; ++g) {
     const grhd2_gpu *h = b->m[g];
     Group *grp = nullptr;
     for (auto &x : b->groups)
       if (x.mixed == h->mixed && x.rec == h->cfg.rec_method && x.rs == h->cfg.riemann) grp = &x;
     if (!grp) {
-      b->groups.push_back(Group{h->mixed, h->cfg.rec_method, h->cfg.riemann, {}, nullptr, {}, {}, {0, 0, 0}});
+      b->groups.push_back(
+          Group{h->mixed, h->cfg.rec_method, h->cfg.riemann, {}, nullptr, {}, {}, {0, 0, 0}, {DEFAULT_TX, DEFAULT_TX, DEFAULT_TX}});
       grp = &b->groups.back();
     }
     grp->members.push_back(g);
   }
+  // flux variant and tile per scheme group and direction; the tiles go into the batch's
+  // copies of the descriptors
+  for (int gi = 0; gi < (int)b->groups.size(); ++gi) {
+    Group &grp = b->groups[gi];
+    for (int d = 1; d <= 3; ++d) {
+      const FluxChoice ch = choose_flux(b, gi, grp, hg, d);
+      grp.variant[d - 1] = ch.variant;
+      grp.tx[d - 1] = ch.tx;
+      for (int g : grp.members) set_face_tiles(hg[g], d, ch.tx);
+    }
+  }
+  BCUDA_TRY(b, cudaMalloc((void **)&b->d_grids, sizeof(GridDev) * n));
+  BCUDA_TRY(b, cudaMalloc((void **)&b->d_clocks, sizeof(GridClock) * n));
+  BCUDA_TRY(b, cudaMemcpyAsync(b->d_grids, hg.data(), sizeof(GridDev) * n, cudaMemcpyHostToDevice, b->stream));
   for (auto &grp : b->groups) {
     std::vector<BlockMap> map;
     for (int k = 0; k < NKIND; ++k) {
@@ -250,7 +325,6 @@ int build_batch(grhd2_gpu_batch *b) {
       }
       grp.nb[k] = (int)map.size() - grp.off[k];
     }
-    for (int d = 0; d < 3; ++d) grp.variant[d] = choose_variant(b, grp, hg, d + 1);
     BCUDA_TRY(b, cudaMalloc((void **)&grp.d_map, sizeof(BlockMap) * std::max<size_t>(1, map.size())));
     BCUDA_TRY(b, cudaMemcpyAsync(grp.d_map, map.data(), sizeof(BlockMap) * map.size(), cudaMemcpyHostToDevice, b->stream));
   }
@@ -545,6 +619,8 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   G.nx = c.nx; G.ny = c.ny; G.nz = c.nz; G.ng = c.nghost; G.case_id = c.case_id;
   G.div_nx = make_fastdiv((unsigned)c.nx); G.div_ny = make_fastdiv((unsigned)c.ny);
   G.div_nx1 = make_fastdiv((unsigned)c.nx + 1); G.div_ny1 = make_fastdiv((unsigned)c.ny + 1);
+  set_cell_tile(G, DEFAULT_TX);
+  for (int d = 1; d <= 3; ++d) set_face_tiles(G, d, DEFAULT_TX);
   G.ncell = (long long)c.nx * c.ny * c.nz;
   G.pplane = (G.ncell + 31) / 32 * 32;
   G.nij = (long long)c.nx * c.ny;
@@ -1166,10 +1242,21 @@ int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant) {
   return build_batch(b);
 }
 
-int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *chosen, int cap, int *n_out) {
+int grhd2_gpu_batch_set_tile(grhd2_gpu_batch *b, int tx) {
+  if (!b) return GRHD2_ERR_ARG;
+  if (tx != 0 && tx != 32 && tx != 64 && tx != 128 && tx != 256)
+    return bfail(b, GRHD2_ERR_ARG, "tile extent %d must be 0 (automatic), 32, 64, 128 or 256", tx);
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  b->tile_request = (unsigned)tx;
+  return build_batch(b);
+}
+
+int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *variants, int *tiles, int cap, int *n_out) {
   if (!b || reps <= 0) return bfail(b, GRHD2_ERR_ARG, "invalid arguments to autotune");
   BCUDA_TRY(b, cudaSetDevice(b->device));
   b->variant_request = GRHD2_FLUX_AUTO;
+  b->tile_request = 0;
+  b->forced.clear();
   if (int rc = build_batch(b)) return rc;
   const int n = (int)b->m.size();
   // tuning launches count reconstruction clamps and HLLC fallbacks: save and restore
@@ -1184,48 +1271,58 @@ int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *chosen, int cap,
   BCUDA_TRY(b, cudaEventCreate(&e0));
   BCUDA_TRY(b, cudaEventCreate(&e1));
   int rc = 0, k = 0;
-  for (auto &grp : b->groups) {
+  const int ngroups = (int)b->groups.size();
+  for (int gi = 0; gi < ngroups && !rc; ++gi) {
     for (int d = 1; d <= 3 && !rc; ++d) {
-      if (grp.nb[K_FLUX_X + d - 1] <= 0) continue;
+      if (b->groups[gi].nb[K_FLUX_X + d - 1] <= 0) continue;
       float best = 0.0f;
-      int best_v = DEFAULT_VARIANT;
+      FluxChoice best_c{DEFAULT_VARIANT, DEFAULT_TX};
+      bool first = true;
       for (int v : {GRHD2_FLUX_SPLIT, GRHD2_FLUX_FUSED}) {
-        auto run = [&]() { return grp.mixed ? enqueue_dir<float, float>(b, grp, d, v) : enqueue_dir<double, double>(b, grp, d, v); };
-        if ((rc = run())) break;  // warm-up
-        cudaEventRecord(e0, b->stream);
-        for (int r = 0; r < reps && !rc; ++r) rc = run();
-        cudaEventRecord(e1, b->stream);
+        for (unsigned tx : {32u, 64u, 128u}) {
+          b->forced[{gi, d}] = FluxChoice{v, tx};
+          if ((rc = build_batch(b))) break;
+          const Group &grp = b->groups[gi];
+          auto run = [&]() {
+            return grp.mixed ? enqueue_dir<float, float>(b, grp, d, v) : enqueue_dir<double, double>(b, grp, d, v);
+          };
+          if ((rc = run())) break;  // warm-up
+          cudaEventRecord(e0, b->stream);
+          for (int r = 0; r < reps && !rc; ++r) rc = run();
+          cudaEventRecord(e1, b->stream);
+          if (rc) break;
+          cudaError_t e = cudaEventSynchronize(e1);
+          if (e != cudaSuccess) { rc = bfail(b, GRHD2_ERR_CUDA, "autotune: %s", cudaGetErrorString(e)); break; }
+          float t = 0.0f;
+          cudaEventElapsedTime(&t, e0, e1);
+          if (first || t < best) { best = t; best_c = FluxChoice{v, tx}; first = false; }
+        }
         if (rc) break;
-        cudaError_t e = cudaEventSynchronize(e1);
-        if (e != cudaSuccess) { rc = bfail(b, GRHD2_ERR_CUDA, "autotune: %s", cudaGetErrorString(e)); break; }
-        float t = 0.0f;
-        cudaEventElapsedTime(&t, e0, e1);
-        if (v == GRHD2_FLUX_SPLIT || t < best) { best = t; best_v = v; }
       }
       if (rc) break;
-      grp.variant[d - 1] = best_v;
+      b->forced[{gi, d}] = best_c;
       {
         std::lock_guard<std::mutex> lock(g_tune_mu);
-        g_tune[tune_key(grp, hg, d)] = best_v;
+        g_tune[tune_key(b->groups[gi], hg, d)] = best_c;
       }
-      if (chosen && k < cap) chosen[k] = best_v;
+      if (k < cap) {
+        if (variants) variants[k] = best_c.variant;
+        if (tiles) tiles[k] = (int)best_c.tx;
+      }
       ++k;
     }
-    if (rc) break;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  b->forced.clear();  // the choices now come from the cache
+  int rc2 = build_batch(b);
   for (int g = 0; g < n; ++g)
     cudaMemcpyAsync(b->m[g]->G.cnt, &saved[(size_t)g * NCNT], NCNT * sizeof(unsigned long long), cudaMemcpyHostToDevice,
                     b->stream);
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (rc) return rc;
+  if (rc2) return rc2;
   if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
-  // the captured step used the previous variants
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->graph) cudaGraphDestroy(b->graph);
-  b->exec = nullptr;
-  b->graph = nullptr;
   if (n_out) *n_out = k;
   return GRHD2_OK;
 }

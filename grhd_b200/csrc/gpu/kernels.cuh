@@ -107,7 +107,7 @@ __device__ __forceinline__ void c2p_count(unsigned long long *cnt, unsigned fl) 
 // MODE 0 writes the RHS only; MODE 1..3 are the SSP-RK3 stages (stage 1 also copies
 // up into u, the "u = up" of grhd2.f90:232).
 // ------------------------------------------------------------------------------------
-// Batched: block b works on grid map[b].grid, cells map[b].first + threadIdx.x.
+// Batched: block b works on grid map[b].grid, cell tile map[b].first / 128.
 // Resident 128-thread blocks per SM the register allocation must allow.  The kernel waits
 // on dependent FP64 chains (con2prim) and scattered table loads, so more warps in flight
 // pay for a few spilled registers: measured on the 2.5D torus batch, 8 blocks (64
@@ -120,8 +120,11 @@ __global__ void __launch_bounds__(128, cell_min_blocks<PT>())
     k_cell_update(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
-  const long long c = (long long)bm.first + threadIdx.x;
-  if (c >= G.ncell) return;
+  unsigned ia, jb, kc;
+  if (!tile_item<7>(G.tiles[TILE_CELL], (unsigned)bm.first >> 7, threadIdx.x, (unsigned)G.nx, (unsigned)G.ny,
+                    (unsigned)G.nz, ia, jb, kc))
+    return;
+  const long long c = (long long)ia + (long long)G.nx * ((long long)jb + (long long)G.ny * kc);
   const Phys P = G.phys;
   PT *__restrict__ Pio = (PT *)G.P;
   const R *__restrict__ Fx = (const R *)G.F[0];
@@ -138,10 +141,7 @@ __global__ void __launch_bounds__(128, cell_min_blocks<PT>())
     dt = clock_dt(ck);
   }
   unsigned long long *cnt = G.cnt;
-  const unsigned r = fdiv((unsigned)c, G.div_nx);
-  const int i0 = (int)((unsigned)c - r * G.div_nx.d);
-  const unsigned kk = fdiv(r, G.div_ny);
-  const int j0 = (int)(r - kk * G.div_ny.d), k0 = (int)kk;
+  const int i0 = (int)ia, j0 = (int)jb, k0 = (int)kc;
   const long long ij = i0 + (long long)G.nx * j0;
   double q[NEQ];
 #pragma unroll

@@ -76,6 +76,31 @@ inline FastDiv make_fastdiv(unsigned d) {
 }
 __device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) { return (__umulhi(n, f.m) + n) >> f.l; }
 
+// Block tile of a stage kernel over its index space (nI, nJ, nK) -- cells, or the faces of
+// one direction.  A block of BS = 2^lb threads covers tx = 2^lx consecutive items along i,
+// ty = 2^ly along j and tz = BS / (tx ty) along k; a warp always spans consecutive i, so
+// loads stay coalesced, while the block's rows along j/k reuse the k-invariant metric
+// tables and the stencil values of their neighbours through L1.  Tiles are numbered with
+// i fastest: t = ti + nti (tj + ntj tk).
+struct Tile {
+  unsigned lx, ly;   // log2 of the tile extent along i and j
+  FastDiv nti, ntj;  // tiles along i and j
+};
+enum TileKind { TILE_CELL = 0, TILE_RECON = 1, TILE_FACE = 4, NTILE = 7 };  // + DIR - 1 for faces
+
+template <int LB>  // log2 of the block size
+__device__ __forceinline__ bool tile_item(const Tile &T, unsigned t, unsigned tid, unsigned nI, unsigned nJ,
+                                          unsigned nK, unsigned &a, unsigned &b, unsigned &c) {
+  const unsigned r = fdiv(t, T.nti);
+  const unsigned ti = t - r * T.nti.d;
+  const unsigned tk = fdiv(r, T.ntj);
+  const unsigned tj = r - tk * T.ntj.d;
+  a = (ti << T.lx) + (tid & ((1u << T.lx) - 1u));
+  b = (tj << T.ly) + ((tid >> T.lx) & ((1u << T.ly) - 1u));
+  c = (tk << (LB - T.lx - T.ly)) + (tid >> (T.lx + T.ly));
+  return a < nI && b < nJ && c < nK;
+}
+
 // Everything a kernel needs about one grid.  The stage kernels read these descriptors from
 // a device array, one entry per grid of a batch (a single grid is a batch of one).
 struct GridDev {
@@ -83,6 +108,7 @@ struct GridDev {
   int nx, ny, nz, ng;
   int case_id;
   FastDiv div_nx, div_ny, div_nx1, div_ny1;  // nx, ny, nx + 1, ny + 1
+  Tile tiles[NTILE];                         // block tiles: cells, recon per direction, faces per direction
   long long ncell;   // nx*ny*nz
   long long pplane;  // plane stride of the primitive / conserved arrays (elements)
   // metric tables

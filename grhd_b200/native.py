@@ -111,7 +111,9 @@ GPU_SYMBOLS = {
     "grhd2_gpu_batch_clocks": (C.c_int, [_VP, c_double_p, C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
     "grhd2_gpu_set_stream": (C.c_int, [_VP, _VP]),
     "grhd2_gpu_device_bytes": (C.c_int64, [C.POINTER(GpuConfig)]),
-    "grhd2_gpu_batch_autotune": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+    "grhd2_gpu_batch_set_tile": (C.c_int, [_VP, C.c_int]),
+    "grhd2_gpu_batch_autotune": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int,
+                                           C.POINTER(C.c_int)]),
     "grhd2_gpu_batch_last_error": (C.c_char_p, [_VP]),
     "grhd2_gpu_batch_destroy": (None, [_VP]),
 }

@@ -76,7 +76,8 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=1, help="replicas stepped as one batch")
     ap.add_argument("--graph", type=int, default=1, help="replay each step as a CUDA graph")
     ap.add_argument("--flux", choices=["auto", "split", "fused", "tune"], default="tune",
-                    help="face-flux kernel variant ('tune': time both on this batch)")
+                    help="face-flux kernel variant ('tune': time variants and tiles on this batch)")
+    ap.add_argument("--tile", type=int, default=0, help="face-kernel tile extent along i (0: automatic)")
     args, rest = ap.parse_known_args(argv)
     overrides = _parse_overrides(rest)
     from .problem import Problem
@@ -111,7 +112,12 @@ def main(argv=None):
     batch = GpuBatch(grids)
     for k in range(len(grids)):
         batch.set_clock(k, 0.0, 1e300, -1)
-    tuned = batch.autotune() if args.flux == "tune" else batch.set_flux_variant(args.flux)
+    if args.flux == "tune":
+        tuned = batch.autotune()
+    else:
+        tuned = None
+        batch.set_flux_variant(args.flux)
+        batch.set_tile(args.tile)
     batch.step(args.warmup, graph=args.graph)
     g.synchronize()
     t0 = time.perf_counter()

@@ -275,15 +275,20 @@ class GpuBatch:
         """'split' (recon + Riemann kernels), 'fused' (one kernel) or 'auto' (tuned/cached)."""
         self._check(self.lib.grhd2_gpu_batch_set_flux_variant(self._b, self.FLUX_VARIANTS[variant]))
 
+    def set_tile(self, tx: int):
+        """Face-kernel block tile extent along i (32, 64, 128, 256; 0 = automatic)."""
+        self._check(self.lib.grhd2_gpu_batch_set_tile(self._b, tx))
+
     def autotune(self, reps: int = 5):
-        """Time both flux variants per scheme group and direction; returns the choices
-        (group order, x before y before z) as variant names."""
+        """Time every (flux variant, tile) pair per scheme group and direction; returns the
+        choices (group order, x before y before z) as (variant name, tile extent)."""
         cap = 64
-        out = (C.c_int * cap)()
+        var = (C.c_int * cap)()
+        til = (C.c_int * cap)()
         n = C.c_int()
-        self._check(self.lib.grhd2_gpu_batch_autotune(self._b, reps, out, cap, C.byref(n)))
+        self._check(self.lib.grhd2_gpu_batch_autotune(self._b, reps, var, til, cap, C.byref(n)))
         names = {v: k for k, v in self.FLUX_VARIANTS.items()}
-        return [names[out[k]] for k in range(min(n.value, cap))]
+        return [(names[var[k]], int(til[k])) for k in range(min(n.value, cap))]
 
     def profile_step(self):
         """[(kernel name, ms)] for every launch of one batched step."""

@@ -209,13 +209,18 @@ int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *a
 #define GRHD2_FLUX_FUSED 1  /* one kernel, thread per face, interface states kept on chip */
 /* Use one variant for every scheme group and direction of the batch (or AUTO). */
 int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant);
-/* Time each variant (reps launches after a warm-up) per scheme group and active direction
- * on the batch's current state and keep the faster one; the choice is also cached for
- * later batches of the same precision, scheme, solver, sensor, direction and size class.
- * The state and counters are left unchanged.  chosen[k] (k < cap) receives the variants in
+/* Block tile of the face kernels: tx consecutive faces along i per block row, the rest of
+ * the block along k (or j for grids without a k extent; the whole block along i for 1D
+ * grids).  tx = 32, 64, 128 or 256; 0 restores the automatic choice. */
+int grhd2_gpu_batch_set_tile(grhd2_gpu_batch *b, int tx);
+/* Time every (variant, tile) pair -- SPLIT or FUSED, tx 32, 64 or 128 -- per scheme group
+ * and active direction (reps launches after a warm-up, on the batch's current state) and
+ * keep the fastest; the choice is also cached for later batches of the same precision,
+ * scheme, solver, sensor, direction and size class.  The state and counters are left
+ * unchanged.  variants[k], tiles[k] (k < cap; either may be NULL) receive the choices in
  * group order, x before y before z; *n_out their number.  Call after the state is set (a
  * grid whose clock is finished does no work and cannot be timed). */
-int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *chosen, int cap, int *n_out);
+int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *variants, int *tiles, int cap, int *n_out);
 const char *grhd2_gpu_batch_last_error(const grhd2_gpu_batch *b);
 void grhd2_gpu_batch_destroy(grhd2_gpu_batch *b);
 /* The handle's CUDA stream (a cudaStream_t) so callers can order their own work and

@@ -40,13 +40,15 @@ def _make(pb, stream, precision="fp64"):
     return g, p0
 
 
-@pytest.mark.parametrize("graph,variant", [(True, "split"), (False, "split"), (True, "fused"), (False, "fused")])
-def test_batch_matches_oracle_per_grid(graph, variant):
+@pytest.mark.parametrize("graph,variant,tile", [(True, "split", 0), (False, "split", 128), (True, "fused", 0),
+                                                (False, "fused", 64), (True, "split", 256)])
+def test_batch_matches_oracle_per_grid(graph, variant, tile):
     s = _stream()
     cases = _cases()
     grids, p0s = zip(*[_make(pb, s) for pb, _, _ in cases])
     b = GpuBatch(list(grids))
     b.set_flux_variant(variant)
+    b.set_tile(tile)
     for k, (pb, tf, ms) in enumerate(cases):
         b.set_clock(k, 0.0, tf, ms)
     # enough replays for the longest grid; finished grids idle
@@ -135,7 +137,8 @@ def test_autotune_leaves_state_and_counters():
         b.set_clock(k, 0.0, 1e30, 4)
     before = [(g.download(want_p=False)[0], g.counters()) for g in grids]
     chosen = b.autotune(reps=2)
-    assert len(chosen) == 3 + 1 and set(chosen) <= {"split", "fused"}
+    assert len(chosen) == 3 + 1
+    assert all(v in ("split", "fused") and t in (32, 64, 128) for v, t in chosen)
     for g, (up, cnt) in zip(grids, before):
         up2 = g.download(want_p=False)[0]
         assert np.array_equal(up, up2) and g.counters() == cnt
