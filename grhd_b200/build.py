@@ -65,12 +65,16 @@ def build_host(force=False, verbose=False) -> str:
 def _precision_flags(src: str):
     """FP64 translation units keep every multiply and add separately rounded (the parity
     path follows the reference's operation order).  The *_fp32.cu units hold only the
-    single-precision reconstruction and Riemann kernels of the mixed policy, whose bar is
-    an L1 tolerance, not bitwise parity: they contract to FMA and use the approximate
-    single-precision division and square root."""
-    if src.endswith("_fp32.cu"):
-        return ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
-    return ["--fmad=false"]
+    single-precision kernels of the mixed policy (reconstruction, Riemann, the cell update
+    with its FP64 con2prim, the persistent step), whose bar is an L1 tolerance, not bitwise
+    parity: they contract to FMA and use the approximate single-precision division and
+    square root."""
+    flags = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"] if "_fp32" in src else ["--fmad=false"]
+    if os.path.basename(src).startswith("persistent_"):
+        # the persistent kernel reads state that other blocks write during the launch:
+        # plain loads bypass L1 (the primitives' loads use ld.global.cg explicitly)
+        flags += ["-Xptxas", "-dlcm=cg"]
+    return flags
 
 
 def build_gpu(force=False, verbose=False) -> str:

@@ -10,8 +10,10 @@ enum CounterIdx { CNT_FLOOR_PRE = 0, CNT_CAUSAL, CNT_BRENT, CNT_ROOT_FAIL, CNT_B
                   CNT_RECON_CLAMP, CNT_HLLC_FALLBACK, NCNT };
 
 // warp-aggregated counter increment (call from converged code)
+// Warp-aggregated counter update: lanes are grouped by counter array (a warp of a
+// persistent kernel can span two grids), one atomic per group.
 __device__ __forceinline__ void count_add(unsigned long long *cnt, int idx, unsigned v) {
-  const unsigned mask = __activemask();
+  const unsigned mask = __match_any_sync(__activemask(), (unsigned long long)cnt);
   const unsigned tot = __reduce_add_sync(mask, v);
   if (tot && (threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(&cnt[idx], (unsigned long long)tot);
 }

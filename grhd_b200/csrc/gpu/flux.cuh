@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const Grid
     base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
   }
   auto ld = [&](int w, int m) -> R {
-    return inside ? R((double)__ldg(&Pin[w * G.pplane + base + m * stride]))
+    return inside ? R((double)GRHD_LDP(&Pin[w * G.pplane + base + m * stride]))
                   : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, w));
   };
   R s[6];
@@ -221,18 +221,16 @@ __global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const Grid
 // ------------------------------------------------------------------------------------
 constexpr int FLUX_BS = 128;
 
+// One face (a, b, c) of direction DIR: all five variables reconstructed, then the Riemann
+// flux.  sq is this thread's column of a [2*NEQ][blockDim] shared array (the rolled
+// variable loop indexes it at run time).
 template <int DIR, int REC, int RS, class R, class PT>
-__global__ void __launch_bounds__(FLUX_BS) k_flux(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
-  __shared__ R sq[2 * NEQ][FLUX_BS];
-  const BlockMap bm = map[blockIdx.x];
-  const GridDev &G = grids[bm.grid];
+__device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned b, unsigned c, R (*sq)[FLUX_BS]) {
+  if (clock_skip(*G.clock)) return;
   const Phys P = G.phys;
   const long long nf = n_faces<DIR>(G);
-  unsigned nI, nJ, nK, a, b, c;
+  unsigned nI, nJ, nK;
   face_space<DIR>(G, nI, nJ, nK);
-  if (!tile_item<7>(G.tiles[TILE_FACE + DIR - 1], (unsigned)bm.first >> 7, threadIdx.x, nI, nJ, nK, a, b, c) ||
-      clock_skip(*G.clock))
-    return;
   const long long f = (long long)a + (long long)nI * ((long long)b + (long long)nJ * c);
   const PT *__restrict__ Pin = (const PT *)G.P;
   const FaceIndex x = face_at<DIR>(G, a, b, c);
@@ -248,7 +246,7 @@ __global__ void __launch_bounds__(FLUX_BS) k_flux(const GridDev *__restrict__ gr
     base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
   }
   auto ld = [&](int v, int m) -> R {
-    return inside ? R((double)__ldg(&Pin[v * G.pplane + base + m * stride]))
+    return inside ? R((double)GRHD_LDP(&Pin[v * G.pplane + base + m * stride]))
                   : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, v));
   };
   int br = BR_GODUNOV;
@@ -302,6 +300,18 @@ __global__ void __launch_bounds__(FLUX_BS) k_flux(const GridDev *__restrict__ gr
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) F[(long long)v * nf + f] = flux[v];
   if (RS == RS_HLLC) count_add(G.cnt, CNT_HLLC_FALLBACK, fb ? 1u : 0u);
+}
+
+
+template <int DIR, int REC, int RS, class R, class PT>
+__global__ void __launch_bounds__(FLUX_BS) k_flux(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+  __shared__ R sq[2 * NEQ][FLUX_BS];
+  const BlockMap bm = map[blockIdx.x];
+  const GridDev &G = grids[bm.grid];
+  unsigned nI, nJ, nK, a, b, c;
+  face_space<DIR>(G, nI, nJ, nK);
+  if (!tile_item<7>(G.tiles[TILE_FACE + DIR - 1], (unsigned)bm.first >> 7, threadIdx.x, nI, nJ, nK, a, b, c)) return;
+  flux_item<DIR, REC, RS, R, PT>(G, a, b, c, sq);
 }
 
 template <int DIR, int RS, class R>

@@ -33,6 +33,41 @@ GRHD_FLUX_EXTERN(2, float, float)
 GRHD_FLUX_EXTERN(3, float, float)
 #undef GRHD_FLUX_EXTERN
 
+// stage cell kernel (cell_fp64.cu / cell_fp32.cu): mode 0 RHS only, 1..3 RK stages
+template <class R, class PT>
+void launch_cell(int mode, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
+extern template void launch_cell<double, double>(int, const GridDev *, const BlockMap *, int, cudaStream_t);
+extern template void launch_cell<float, float>(int, const GridDev *, const BlockMap *, int, cudaStream_t);
+
+// persistent step kernel (persistent.cuh): one contiguous range of items of a phase --
+// the faces of one direction of one grid (dir 1..3) or the cells of one grid (dir 0)
+struct Segment {
+  int grid, dir;
+  long long first, count;
+};
+struct PersistentArgs {
+  const GridDev *grids;
+  const int *members;
+  int nmembers;
+  const Segment *seg_face;
+  int nseg_face;
+  long long n_face;
+  const Segment *seg_cell;
+  int nseg_cell;
+  long long n_cell;
+  unsigned *bar;     // barrier words: arrivals, generation
+  unsigned *status;  // nonzero: a barrier timed out
+};
+// query: *max_blocks = resident blocks of the (rec, rs) instantiation; else launch nsteps
+// steps on nblocks blocks (cooperative launch)
+template <class R, class PT>
+cudaError_t run_persistent(int rec, int rs, bool query, int *max_blocks, const PersistentArgs &a, int nsteps,
+                           int nblocks, cudaStream_t s);
+extern template cudaError_t run_persistent<double, double>(int, int, bool, int *, const PersistentArgs &, int, int,
+                                                           cudaStream_t);
+extern template cudaError_t run_persistent<float, float>(int, int, bool, int *, const PersistentArgs &, int, int,
+                                                         cudaStream_t);
+
 // fused face fluxes of direction dir (recon + Riemann in one kernel)
 template <class R, class PT>
 inline void launch_flux(int dir, int rec, int rs, const GridDev *grids, const BlockMap *map, int nblocks,

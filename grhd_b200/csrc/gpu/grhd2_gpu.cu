@@ -148,6 +148,12 @@ struct Group {
   int off[NKIND], nb[NKIND];
   int variant[3];  // per direction: GRHD2_FLUX_SPLIT or GRHD2_FLUX_FUSED
   unsigned tx[3];  // per direction: tile extent along i of the face kernels
+  // persistent step kernel: member list and the item segments of its two phases
+  int *d_members = nullptr;
+  Segment *d_seg = nullptr;  // face segments, then cell segments
+  int nseg_face = 0, nseg_cell = 0;
+  long long n_face = 0, n_cell = 0;
+  int max_blocks = 0;  // resident blocks of the group's persistent instantiation
 };
 
 struct FluxChoice {
@@ -165,6 +171,9 @@ struct grhd2_gpu_batch {
   std::vector<Group> groups;
   int variant_request = GRHD2_FLUX_AUTO;  // GRHD2_FLUX_AUTO: tuned choice if cached, else the default
   unsigned tile_request = 0;              // 0: tuned tile if cached, else DEFAULT_TX
+  int step_request = GRHD2_STEP_AUTO;     // stage kernels in a graph, or the persistent kernel
+  bool persistent = false;                // the mode in use
+  unsigned *d_bar = nullptr;              // persistent kernel barrier words and status
   std::map<std::pair<int, int>, FluxChoice> forced;  // (group, direction) -> choice, while tuning
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -235,7 +244,13 @@ void destroy_batch_resources(grhd2_gpu_batch *b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
-  for (auto &g : b->groups) if (g.d_map) cudaFree(g.d_map);
+  for (auto &g : b->groups) {
+    if (g.d_map) cudaFree(g.d_map);
+    if (g.d_members) cudaFree(g.d_members);
+    if (g.d_seg) cudaFree(g.d_seg);
+  }
+  if (b->d_bar) cudaFree(b->d_bar);
+  b->d_bar = nullptr;
   b->groups.clear();
   if (b->d_grids) cudaFree(b->d_grids);
   b->d_grids = nullptr;
@@ -267,6 +282,11 @@ TuneKey tune_key(const Group &grp, const std::vector<GridDev> &hg, int dir) {
 
 // default without tuning: the split kernels (recon at high occupancy, lean Riemann)
 constexpr int DEFAULT_VARIANT = GRHD2_FLUX_SPLIT;
+// Automatic step mode: the graph of stage kernels.  Measured on one B200 with 1024-cell 1D
+// grids, a graph replay takes 83-88 us per step and the persistent kernel 127-135 us: a
+// small grid is bound by the dependent arithmetic chain of one item per thread, not by
+// launch latency (graph replays hide the gaps), and the persistent kernel's fused face
+// phase reconstructs the five variables of a face in one thread, one after the other.
 
 FluxChoice choose_flux(const grhd2_gpu_batch *b, int gi, const Group &grp, const std::vector<GridDev> &hg, int dir) {
   auto f = b->forced.find({gi, dir});
@@ -327,7 +347,40 @@ int build_batch(grhd2_gpu_batch *b) {
     }
     BCUDA_TRY(b, cudaMalloc((void **)&grp.d_map, sizeof(BlockMap) * std::max<size_t>(1, map.size())));
     BCUDA_TRY(b, cudaMemcpyAsync(grp.d_map, map.data(), sizeof(BlockMap) * map.size(), cudaMemcpyHostToDevice, b->stream));
+    // persistent kernel: flattened item spaces (faces of every active direction; cells)
+    std::vector<Segment> seg;
+    long long first = 0;
+    for (int g : grp.members)
+      for (int d = 1; d <= 3; ++d)
+        if (dir_active(hg[g], d)) {
+          seg.push_back(Segment{g, d, first, face_count(hg[g], d)});
+          first += face_count(hg[g], d);
+        }
+    grp.nseg_face = (int)seg.size();
+    grp.n_face = first;
+    first = 0;
+    for (int g : grp.members) {
+      seg.push_back(Segment{g, 0, first, hg[g].ncell});
+      first += hg[g].ncell;
+    }
+    grp.nseg_cell = (int)seg.size() - grp.nseg_face;
+    grp.n_cell = first;
+    BCUDA_TRY(b, cudaMalloc((void **)&grp.d_seg, sizeof(Segment) * seg.size()));
+    BCUDA_TRY(b, cudaMemcpyAsync(grp.d_seg, seg.data(), sizeof(Segment) * seg.size(), cudaMemcpyHostToDevice, b->stream));
+    BCUDA_TRY(b, cudaMalloc((void **)&grp.d_members, sizeof(int) * grp.members.size()));
+    BCUDA_TRY(b, cudaMemcpyAsync(grp.d_members, grp.members.data(), sizeof(int) * grp.members.size(),
+                                 cudaMemcpyHostToDevice, b->stream));
+    cudaError_t e = grp.mixed ? run_persistent<float, float>(grp.rec, grp.rs, true, &grp.max_blocks, {}, 0, 0, b->stream)
+                              : run_persistent<double, double>(grp.rec, grp.rs, true, &grp.max_blocks, {}, 0, 0, b->stream);
+    if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "persistent kernel occupancy: %s", cudaGetErrorString(e));
   }
+  BCUDA_TRY(b, cudaMalloc((void **)&b->d_bar, 4 * sizeof(unsigned)));
+  BCUDA_TRY(b, cudaMemsetAsync(b->d_bar, 0, 4 * sizeof(unsigned), b->stream));
+  // step mode
+  b->persistent = b->step_request == GRHD2_STEP_PERSISTENT;
+  if (b->persistent)
+    for (const auto &grp : b->groups)
+      if (grp.max_blocks <= 0) return bfail(b, GRHD2_ERR_CUDA, "the persistent step kernel cannot be resident");
   BCUDA_TRY(b, cudaStreamSynchronize(b->stream));  // host vectors go out of scope
   return 0;
 }
@@ -370,7 +423,7 @@ int enqueue_fluxes(grhd2_gpu_batch *b, const Group &grp) {
 template <int MODE, class R, class PT>
 int enqueue_cells(grhd2_gpu_batch *b, const Group &grp) {
   if (grp.nb[K_CELL] <= 0) return 0;
-  k_cell_update<MODE, R, PT><<<grp.nb[K_CELL], CELL_BS, 0, b->stream>>>(b->d_grids, grp.d_map + grp.off[K_CELL]);
+  launch_cell<R, PT>(MODE, b->d_grids, grp.d_map + grp.off[K_CELL], grp.nb[K_CELL], b->stream);
   return blaunch_check(b, MODE == 0 ? "cell_rhs" : "cell_update");
 }
 
@@ -395,12 +448,44 @@ int enqueue_step(grhd2_gpu_batch *b) {
   return blaunch_check(b, "advance_clocks");
 }
 
+// nsteps whole steps of every scheme group, each group one cooperative launch of the
+// persistent kernel (groups run one after the other on the batch stream)
+int enqueue_persistent(grhd2_gpu_batch *b, long long nsteps) {
+  for (const auto &grp : b->groups) {
+    const PersistentArgs a{b->d_grids, grp.d_members, (int)grp.members.size(), grp.d_seg, grp.nseg_face, grp.n_face,
+                           grp.d_seg + grp.nseg_face, grp.nseg_cell, grp.n_cell, b->d_bar, b->d_bar + 2};
+    const long long need = std::max(std::max(grp.n_face, grp.n_cell), (long long)grp.members.size());
+    const int blocks = (int)std::max(1LL, std::min<long long>(grp.max_blocks, (need + FUSED_FLUX_BS - 1) / FUSED_FLUX_BS));
+    for (long long done = 0; done < nsteps;) {
+      const int chunk = (int)std::min<long long>(nsteps - done, 1 << 30);
+      BCUDA_TRY(b, cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), b->stream));  // arrivals, generation
+      cudaError_t e = grp.mixed ? run_persistent<float, float>(grp.rec, grp.rs, false, nullptr, a, chunk, blocks, b->stream)
+                                : run_persistent<double, double>(grp.rec, grp.rs, false, nullptr, a, chunk, blocks, b->stream);
+      if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "persistent step kernel launch: %s", cudaGetErrorString(e));
+      if (int rc = blaunch_check(b, "persistent_step")) return rc;
+      done += chunk;
+    }
+  }
+  return 0;
+}
+
+// the persistent kernel's status word (nonzero: a grid barrier timed out); synchronises
+int check_persistent(grhd2_gpu_batch *b) {
+  if (!b->d_bar) return 0;
+  unsigned st = 0;
+  BCUDA_TRY(b, cudaMemcpyAsync(&st, b->d_bar + 2, sizeof st, cudaMemcpyDeviceToHost, b->stream));
+  BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  if (st) return bfail(b, GRHD2_ERR_CUDA, "persistent step kernel: a grid barrier timed out (status %u)", st);
+  return 0;
+}
+
 int batch_steps(grhd2_gpu_batch *b, long long nsteps, bool use_graph) {
   for (size_t g = 0; g < b->m.size(); ++g)
     if (b->m[g]->stream != b->stream)
       return bfail(b, GRHD2_ERR_STATE, "grid %zu moved to another stream after the batch was created", g);
   if (int rc = refresh_batch(b)) return rc;
   if (nsteps <= 0) return 0;
+  if (b->persistent) return enqueue_persistent(b, nsteps);
   if (!use_graph) {
     for (long long s = 0; s < nsteps; ++s)
       if (int rc = enqueue_step(b)) return rc;
@@ -482,7 +567,7 @@ int profile_common(grhd2_gpu_batch *b, float *ms, const char **names, int cap, i
   BCUDA_TRY(b, cudaEventRecord(start, b->stream));
   b->profiling = true;
   int rc = refresh_batch(b);
-  if (!rc) rc = enqueue_step(b);
+  if (!rc) rc = b->persistent ? enqueue_persistent(b, 1) : enqueue_step(b);
   b->profiling = false;
   cudaError_t e = cudaStreamSynchronize(b->stream);
   const int n = (int)b->prof_ev.size();
@@ -884,6 +969,7 @@ int grhd2_gpu_run(grhd2_gpu *h, double t0, double final_time, int64_t max_steps,
   if (int rc = batch_steps(h->self, n, true)) return fail(h, rc, "%s", h->self->err.c_str());
   CUDA_TRY(h, cudaMemcpyAsync(&h->hclock, h->G.clock, sizeof(GridClock), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (int rc = check_persistent(h->self)) return fail(h, rc, "%s", h->self->err.c_str());
   if (h->hclock.steps != pred.steps || h->hclock.t != pred.t)
     return fail(h, GRHD2_ERR_STATE, "device clock (%lld steps) differs from the host prediction (%lld)",
                 (long long)h->hclock.steps, (long long)pred.steps);
@@ -1209,6 +1295,7 @@ int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *ste
   GridClock c;
   BCUDA_TRY(b, cudaMemcpyAsync(&c, h->G.clock, sizeof c, cudaMemcpyDeviceToHost, b->stream));
   BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  if (int rc = check_persistent(b)) return rc;
   if (t) *t = c.t;
   if (steps) *steps = c.steps;
   if (active) *active = c.active;
@@ -1225,6 +1312,7 @@ int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *a
   if (int rc = blaunch_check(b, "gather_clocks")) return rc;
   BCUDA_TRY(b, cudaMemcpyAsync(c.data(), b->d_clocks, sizeof(GridClock) * n, cudaMemcpyDeviceToHost, b->stream));
   BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  if (int rc = check_persistent(b)) return rc;
   for (int g = 0; g < n; ++g) {
     if (t) t[g] = c[g].t;
     if (steps) steps[g] = c[g].steps;
@@ -1240,6 +1328,21 @@ int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant) {
   BCUDA_TRY(b, cudaSetDevice(b->device));
   b->variant_request = variant;
   return build_batch(b);
+}
+
+int grhd2_gpu_batch_set_step_mode(grhd2_gpu_batch *b, int mode) {
+  if (!b) return GRHD2_ERR_ARG;
+  if (mode != GRHD2_STEP_AUTO && mode != GRHD2_STEP_GRAPH && mode != GRHD2_STEP_PERSISTENT)
+    return bfail(b, GRHD2_ERR_ARG, "invalid step mode %d", mode);
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  b->step_request = mode;
+  return build_batch(b);
+}
+
+int grhd2_gpu_batch_step_mode(grhd2_gpu_batch *b) {
+  if (!b) return GRHD2_ERR_ARG;
+  if (int rc = refresh_batch(b)) return rc;
+  return b->persistent ? GRHD2_STEP_PERSISTENT : GRHD2_STEP_GRAPH;
 }
 
 int grhd2_gpu_batch_set_tile(grhd2_gpu_batch *b, int tx) {

@@ -59,6 +59,27 @@ __host__ __device__ __forceinline__ double clock_dt(const GridClock &c) {
   return (c.t + c.dt_cfl > c.final_time) ? c.final_time - c.t : c.dt_cfl;
 }
 __host__ __device__ __forceinline__ bool clock_skip(const GridClock &c) { return c.mode == 1 && !c.active; }
+// end of a step: t = t + dt, steps += 1 (grhd2.f90:229-230); a grid that reached its final
+// time or step limit deactivates
+__device__ __forceinline__ void advance_clock(GridClock *c) {
+  if (c->mode == 1) {
+    if (!c->active) return;
+    c->t = c->t + clock_dt(*c);
+    c->steps += 1;
+    c->active = c->t < c->final_time && (c->max_steps < 0 || c->steps < c->max_steps);
+  } else {
+    c->steps += 1;
+  }
+}
+
+// Loads of the primitives.  Within one stage kernel they are read-only (the non-coherent
+// read-only path is safe); the persistent step kernel writes them between its phases, so
+// its translation units read them through L2 (ld.global.cg), coherent across blocks.
+#ifdef GRHD_PERSISTENT_TU
+#define GRHD_LDP(ptr) __ldcg(ptr)
+#else
+#define GRHD_LDP(ptr) __ldg(ptr)
+#endif
 
 // Division by a grid extent with a multiply-high and a shift (Granlund and Montgomery,
 // "Division by invariant integers using multiplication", 1994): for d >= 1 with
@@ -148,13 +169,13 @@ __device__ __forceinline__ unsigned cell_index(const GridDev &G, int i, int j, i
 template <class PT>
 __device__ __forceinline__ double ld_prim(const PT *__restrict__ P, const GridDev &G, int v, int i, int j, int k) {
   const unsigned c = cell_index(G, i, j, k);
-  return (double)__ldg(&P[v * G.pplane + c]);
+  return (double)GRHD_LDP(&P[v * G.pplane + c]);
 }
 template <class PT>
 __device__ __forceinline__ void ld_cell(const PT *__restrict__ P, const GridDev &G, int i, int j, int k, double (&q)[NEQ]) {
   const unsigned c = cell_index(G, i, j, k);
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v) q[v] = (double)__ldg(&P[v * G.pplane + c]);
+  for (int v = 0; v < NEQ; ++v) q[v] = (double)GRHD_LDP(&P[v * G.pplane + c]);
 }
 __device__ __forceinline__ int wrap(int i, int n) {  // periodic (whole-array statements per g) == modular
   int r = (i - 1) % n;

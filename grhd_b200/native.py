@@ -112,6 +112,8 @@ GPU_SYMBOLS = {
     "grhd2_gpu_set_stream": (C.c_int, [_VP, _VP]),
     "grhd2_gpu_device_bytes": (C.c_int64, [C.POINTER(GpuConfig)]),
     "grhd2_gpu_batch_set_tile": (C.c_int, [_VP, C.c_int]),
+    "grhd2_gpu_batch_set_step_mode": (C.c_int, [_VP, C.c_int]),
+    "grhd2_gpu_batch_step_mode": (C.c_int, [_VP]),
     "grhd2_gpu_batch_autotune": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int,
                                            C.POINTER(C.c_int)]),
     "grhd2_gpu_batch_last_error": (C.c_char_p, [_VP]),

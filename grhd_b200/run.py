@@ -66,6 +66,57 @@ def _parse_overrides(rest):
     return out
 
 
+def michel_l1(pb, p) -> float:
+    """The reference's Michel error (output.f90:1189-1213): mean |rho - rho_exact| over
+    cells i = int(0.10 nx) .. int(0.95 nx) (1-based), rho_exact the analytic steady
+    profile the run starts from (before any perturbation)."""
+    import numpy as np
+    g, nx = pb.ng, pb.nx
+    exact = pb.initial_prims()
+    i0 = max(1, int(0.10 * nx))
+    i1 = min(nx, max(i0, int(0.95 * nx)))
+    rows = slice(g + i0, g + i1 + 1)  # array index of cell i is g + i
+    j, k = g + 1, g + 1
+    return float(np.abs(p[k, j, rows, 0] - exact[k, j, rows, 0]).mean())
+
+
+def accuracy_run(pb, p0, final_time, max_steps):
+    """FP64 and mixed runs of one problem from the same state (each on its own device
+    clock: CFL dt clamped to final_time, or max_steps steps)."""
+    import numpy as np
+    from .solver import GpuBatch, GpuGrid
+    tf = final_time if final_time is not None else 1e300
+    ms = -1 if final_time is not None else max_steps
+    out = {"cells": pb.n_cells, "final_time": final_time}
+    ups, ps = {}, {}
+    for prec in ("fp64", "mixed"):
+        g = GpuGrid(pb, precision=prec, upload_initial=False)
+        g.upload(p=p0)
+        g.prim_to_cons()
+        b = GpuBatch([g])
+        b.set_clock(0, 0.0, tf, ms)
+        t0 = time.perf_counter()
+        while b.clock(0)[2]:
+            b.step(2000, graph=True)
+        el = time.perf_counter() - t0
+        t, n, _ = b.clock(0)
+        up, pp = g.download(p_template=p0)
+        ups[prec], ps[prec] = up, pp
+        out[prec] = {"steps": int(n), "t": t, "seconds": el, "zone_updates_per_s": pb.n_cells * n / el,
+                     "counters": g.counters()}
+        if pb.info.case_id == 7:
+            out[prec]["michel_l1_vs_analytic"] = michel_l1(pb, pp)
+        b.close()
+        g.close()
+    a, r = ups["mixed"].reshape(-1, 5), ups["fp64"].reshape(-1, 5)
+    den = np.abs(r).sum(axis=0)
+    num = np.abs(a - r).sum(axis=0)
+    out["l1_mixed_vs_fp64"] = np.where(den > 0, num / np.where(den > 0, den, 1.0), num).tolist()
+    # momentum components measured against the whole momentum (one may be ~0 by symmetry)
+    out["l1_mixed_vs_fp64_momentum_norm"] = (num[2:5] / np.abs(r[:, 2:5]).sum()).tolist()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--par", help=".par file")
@@ -78,6 +129,10 @@ def main(argv=None):
     ap.add_argument("--flux", choices=["auto", "split", "fused", "tune"], default="tune",
                     help="face-flux kernel variant ('tune': time variants and tiles on this batch)")
     ap.add_argument("--tile", type=int, default=0, help="face-kernel tile extent along i (0: automatic)")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="run the problem in FP64 and mixed from the same state to --final-time (or --steps) "
+                         "and report the mixed-vs-FP64 L1 (and the Michel L1 against the analytic profile)")
+    ap.add_argument("--final-time", type=float, default=None)
     args, rest = ap.parse_known_args(argv)
     overrides = _parse_overrides(rest)
     from .problem import Problem
@@ -94,6 +149,9 @@ def main(argv=None):
     p = pb.initial_prims()
     if pb.info.perturbation_type and pb.info.perturbation_time <= 0.0:
         pb.perturb(p)
+    if args.accuracy:
+        print(json.dumps(accuracy_run(pb, p, args.final_time, args.steps)))
+        return 0
     # replicas of the problem, each with its own perturbation seed, on one stream
     grids = []
     for r in range(max(1, args.batch)):

@@ -275,6 +275,20 @@ class GpuBatch:
         """'split' (recon + Riemann kernels), 'fused' (one kernel) or 'auto' (tuned/cached)."""
         self._check(self.lib.grhd2_gpu_batch_set_flux_variant(self._b, self.FLUX_VARIANTS[variant]))
 
+    STEP_MODES = {"auto": -1, "graph": 0, "persistent": 1}
+
+    def set_step_mode(self, mode: str):
+        """'graph' (stage kernels replayed as a CUDA graph), 'persistent' (one cooperative
+        launch per scheme group runs whole steps) or 'auto' (the library's choice: graph)."""
+        self._check(self.lib.grhd2_gpu_batch_set_step_mode(self._b, self.STEP_MODES[mode]))
+
+    @property
+    def step_mode(self) -> str:
+        rc = self.lib.grhd2_gpu_batch_step_mode(self._b)
+        if rc < 0:
+            self._check(rc)
+        return "persistent" if rc == 1 else "graph"
+
     def set_tile(self, tx: int):
         """Face-kernel block tile extent along i (32, 64, 128, 256; 0 = automatic)."""
         self._check(self.lib.grhd2_gpu_batch_set_tile(self._b, tx))

@@ -209,6 +209,14 @@ int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *a
 #define GRHD2_FLUX_FUSED 1  /* one kernel, thread per face, interface states kept on chip */
 /* Use one variant for every scheme group and direction of the batch (or AUTO). */
 int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant);
+/* How a batch runs its steps. */
+#define GRHD2_STEP_AUTO -1       /* the library's choice (currently GRAPH, the faster on every size measured) */
+#define GRHD2_STEP_GRAPH 0       /* the stage kernels (recon, Riemann, cell update per stage), one CUDA graph */
+#define GRHD2_STEP_PERSISTENT 1  /* one cooperative launch per scheme group runs whole steps: fused
+                                    face fluxes and cell updates separated by grid barriers */
+int grhd2_gpu_batch_set_step_mode(grhd2_gpu_batch *b, int mode);
+/* The mode in use (GRHD2_STEP_GRAPH or GRHD2_STEP_PERSISTENT), or a negative error. */
+int grhd2_gpu_batch_step_mode(grhd2_gpu_batch *b);
 /* Block tile of the face kernels: tx consecutive faces along i per block row, the rest of
  * the block along k (or j for grids without a k extent; the whole block along i for 1D
  * grids).  tx = 32, 64, 128 or 256; 0 restores the automatic choice. */

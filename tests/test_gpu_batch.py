@@ -40,15 +40,18 @@ def _make(pb, stream, precision="fp64"):
     return g, p0
 
 
-@pytest.mark.parametrize("graph,variant,tile", [(True, "split", 0), (False, "split", 128), (True, "fused", 0),
-                                                (False, "fused", 64), (True, "split", 256)])
-def test_batch_matches_oracle_per_grid(graph, variant, tile):
+@pytest.mark.parametrize("graph,variant,tile,mode", [
+    (True, "split", 0, "graph"), (False, "split", 128, "graph"), (True, "fused", 0, "graph"),
+    (False, "fused", 64, "graph"), (True, "split", 256, "graph"), (True, "split", 0, "persistent")])
+def test_batch_matches_oracle_per_grid(graph, variant, tile, mode):
     s = _stream()
     cases = _cases()
     grids, p0s = zip(*[_make(pb, s) for pb, _, _ in cases])
     b = GpuBatch(list(grids))
     b.set_flux_variant(variant)
     b.set_tile(tile)
+    b.set_step_mode(mode)
+    assert b.step_mode == mode
     for k, (pb, tf, ms) in enumerate(cases):
         b.set_clock(k, 0.0, tf, ms)
     # enough replays for the longest grid; finished grids idle
@@ -71,6 +74,39 @@ def test_batch_matches_oracle_per_grid(graph, variant, tile):
         for key in ("c2p_floor_pre", "c2p_causal_rescale", "c2p_brent_used", "c2p_root_fail", "c2p_bad_V",
                     "c2p_final_sanitise"):
             assert co[key] == cg[key], f"grid {k} counter {key}"
+    b.close()
+    for g in grids:
+        g.close()
+
+
+@pytest.mark.parametrize("mode", ["graph", "persistent"])
+def test_step_modes_agree(mode):
+    """The persistent step kernel and the graph of stage kernels give bit-identical FP64
+    states, clocks and counters (both against a solo run in the other mode)."""
+    s = _stream()
+    pbs = [torus_3d(nx=24, ny=12, nz=12), michel(nx=200), shock_tube(nx=333, rec="mp5", rs="hllc")]
+    other = "graph" if mode == "persistent" else "persistent"
+    ref = []
+    for pb in pbs:
+        g, _ = _make(pb, s)
+        b1 = GpuBatch([g])
+        b1.set_step_mode(other)
+        b1.set_clock(0, 0.0, 1e30, 9)
+        b1.step(12)
+        ref.append((g.download(want_p=False)[0], g.counters(), b1.clock(0)))
+        b1.close()
+        g.close()
+    grids = [_make(pb, s)[0] for pb in pbs]
+    b = GpuBatch(grids)
+    b.set_step_mode(mode)
+    for k in range(len(grids)):
+        b.set_clock(k, 0.0, 1e30, 9)
+    b.step(5)
+    b.step(7)
+    for k, g in enumerate(grids):
+        assert b.clock(k) == ref[k][2]
+        assert np.array_equal(g.download(want_p=False)[0], ref[k][0])
+        assert g.counters() == ref[k][1]
     b.close()
     for g in grids:
         g.close()
@@ -106,6 +142,7 @@ def test_batch_profile_names():
     s = _stream()
     grids = [_make(pb, s)[0] for pb in (torus_3d(nx=16, ny=8, nz=8), shock_tube(nx=64))]
     b = GpuBatch(grids)
+    b.set_step_mode("graph")
     b.set_flux_variant("split")
     for k in range(2):
         b.set_clock(k, 0.0, 1e30, 1)
@@ -115,6 +152,8 @@ def test_batch_profile_names():
     b.set_flux_variant("fused")
     names = [n for n, _ in b.profile_step()]
     assert names.count("flux_x") == 3 * 2 and names.count("flux_z") == 3 and "recon_x" not in names
+    b.set_step_mode("persistent")
+    assert [n for n, _ in b.profile_step()] == ["persistent_step"] * 2  # one launch per scheme group
     b.close()
     for g in grids:
         g.close()
@@ -133,6 +172,7 @@ def test_autotune_leaves_state_and_counters():
         g.close()
     grids = [_make(pb, s)[0] for pb in pbs]
     b = GpuBatch(grids)
+    b.set_step_mode("graph")
     for k in range(len(grids)):
         b.set_clock(k, 0.0, 1e30, 4)
     before = [(g.download(want_p=False)[0], g.counters()) for g in grids]
