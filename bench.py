@@ -64,6 +64,17 @@ def dist_env():
     return rank, world, local
 
 
+def reduce_max(value: float, world: int, device: str = "cuda") -> float:
+    """Maximum of a per-rank value over all ranks (the job's time is its slowest rank)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -195,13 +206,9 @@ def run_ours(args):
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def max_over_ranks(ms):
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return reduce_max(ms, world, "cuda")
 
-    def timed(b, flush):
+    def timed(b, flush, tag):
         """ms of args.steps batched steps (graph replays), CUDA events on the batch's stream."""
         b.step(args.warmup, graph=True)
         torch.cuda.synchronize()
@@ -209,6 +216,7 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push(f"timed_{tag}")  # lets a profiler select the timed launches
         for s in range(args.steps):
             if flush:
                 with torch.cuda.stream(stream):
@@ -216,16 +224,17 @@ def run_ours(args):
             evs[s][0].record(stream)
             b.step(1, graph=True)
             evs[s][1].record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         return max_over_ranks(sum(a.elapsed_time(c) for a, c in evs))
 
     nb = args.batch
     with ClockSampler(local) as clk:
         g64, b64 = make_batch(nb, "fp64", stream)
-        ms64 = timed(b64, flush=False)
+        ms64 = timed(b64, flush=False, tag="fp64_batched")
     clocks = clk.summary()
     gmx, bmx = make_batch(nb, "mixed", stream)
-    msmx = timed(bmx, flush=False)
+    msmx = timed(bmx, flush=False, tag="mixed_batched")
     # L1 of the mixed policy against FP64 after the same steps from the same state
     up64 = g64[0].download(want_p=False)[0]
     upmx = gmx[0].download(want_p=False)[0]
@@ -241,7 +250,7 @@ def run_ours(args):
     singles = {}
     for prec in ("fp64", "mixed"):
         gs, bs = make_batch(1, prec, stream)
-        ms = timed(bs, flush=True)
+        ms = timed(bs, flush=True, tag=f"{prec}_single")
         singles[prec] = {"value": world * ncell * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps}
         close_batch(gs, bs)
 
