@@ -16,7 +16,7 @@ __device__ __forceinline__ void sources(const GridDev &G, const Phys &P, long lo
 #pragma unroll
   for (int n = 0; n < NEQ; ++n) src[n] = R(0);
   if (P.srhd) return;
-  const double *__restrict__ C = G.centre;
+  const R *__restrict__ C = centre_table<R>(G);
   const long long S = G.nij;
   auto ld = [&](int fld) { return R(__ldg(&C[fld * S + ij])); };
   const R alpha = ld(CF_ALPHA), sqg = ld(CF_SQG);

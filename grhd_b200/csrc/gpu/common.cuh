@@ -18,8 +18,8 @@ __device__ __forceinline__ void count_add(unsigned long long *cnt, int idx, unsi
   if (tot && (threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(&cnt[idx], (unsigned long long)tot);
 }
 
-template <class R>
-__device__ __forceinline__ FaceMetric<R> load_face_metric(const double *__restrict__ T, long long nf, long long f) {
+template <class R, class TT>
+__device__ __forceinline__ FaceMetric<R> load_face_metric(const TT *__restrict__ T, long long nf, long long f) {
   FaceMetric<R> m;
   m.alpha = R(__ldg(&T[FF_ALPHA * nf + f]));
   m.beta_n = R(__ldg(&T[FF_BETA_N * nf + f]));
@@ -29,15 +29,15 @@ __device__ __forceinline__ FaceMetric<R> load_face_metric(const double *__restri
   m.gup = R(__ldg(&T[FF_GUP * nf + f]));
   return m;
 }
-template <class R>
-__device__ __forceinline__ FaceFrame<R> load_face_frame(const double *__restrict__ T, long long nf, long long f) {
+template <class R, class TT>
+__device__ __forceinline__ FaceFrame<R> load_face_frame(const TT *__restrict__ T, long long nf, long long f) {
   FaceFrame<R> fr;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int i = 0; i < 3; ++i) fr.cof[a][i] = R(__ldg(&T[(FF_COF + 3 * a + i) * nf + f]));
   fr.gup = R(__ldg(&T[FF_GUP * nf + f]));
-  fr.ok = __ldg(&T[FF_FRAME_OK * nf + f]) != 0.0;
+  fr.ok = __ldg(&T[FF_FRAME_OK * nf + f]) != TT(0);
   return fr;
 }
 

@@ -281,10 +281,10 @@ __device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) { qL[v] = sq[v][threadIdx.x]; qR[v] = sq[NEQ + v][threadIdx.x]; }
   R *__restrict__ F = (R *)G.F[DIR - 1];
-  const double *T = G.face[DIR - 1];
+  const R *T = face_table<R>(G, DIR - 1);
   const long long ntab = G.nface[DIR - 1];
   bool fb = false;
-  if (__ldg(&T[FF_ZERO * ntab + x.ft]) != 0.0) {
+  if (__ldg(&T[FF_ZERO * ntab + x.ft]) != R(0)) {
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) flux[v] = R(0);
   } else {
@@ -333,10 +333,10 @@ __global__ void __launch_bounds__(128, GRHD_RIEMANN_MIN_BLOCKS) k_riemann(const 
   R qL[NEQ], qR[NEQ], flux[NEQ];
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) { qL[v] = Q[(long long)v * nf + f]; qR[v] = Q[(long long)(5 + v) * nf + f]; }
-  const double *T = G.face[DIR - 1];
+  const R *T = face_table<R>(G, DIR - 1);
   const long long ntab = G.nface[DIR - 1];
   bool fb = false;
-  if (__ldg(&T[FF_ZERO * ntab + x.ft]) != 0.0) {
+  if (__ldg(&T[FF_ZERO * ntab + x.ft]) != R(0)) {
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) flux[v] = R(0);
   } else {

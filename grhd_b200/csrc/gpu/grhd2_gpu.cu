@@ -127,6 +127,7 @@ struct grhd2_gpu {
   cudaStream_t stream = nullptr;
   // owned device buffers (their addresses are also in G)
   double *centre = nullptr, *face[3] = {nullptr, nullptr, nullptr};
+  float *centre_f = nullptr, *face_f[3] = {nullptr, nullptr, nullptr};  // mixed policy only
   double *inj = nullptr, *dust = nullptr, *xc = nullptr, *frozen[3] = {nullptr, nullptr, nullptr};
   unsigned long long *red = nullptr;
   double *staging = nullptr;
@@ -618,10 +619,13 @@ long long handle_bytes(const grhd2_gpu_config &c) {
     a.push_back(5LL * c.nx * c.nz * 8);
     a.push_back(5LL * c.nx * c.ny * 8);
   }
-  a.push_back((long long)NCF * c.nx * c.ny * 8);
-  a.push_back((long long)NFF * (c.nx + 1) * c.ny * 8);
-  if (c.ny > 1) a.push_back((long long)NFF * c.nx * (c.ny + 1) * 8);
-  if (c.nz > 1) a.push_back((long long)NFF * c.nx * c.ny * 8);
+  for (long long tb : {8LL, c.precision_policy == GRHD2_PREC_MIXED ? 4LL : 0LL}) {  // tables (+ FP32 copies)
+    if (tb == 0) continue;
+    a.push_back((long long)NCF * c.nx * c.ny * tb);
+    a.push_back((long long)NFF * (c.nx + 1) * c.ny * tb);
+    if (c.ny > 1) a.push_back((long long)NFF * c.nx * (c.ny + 1) * tb);
+    if (c.nz > 1) a.push_back((long long)NFF * c.nx * c.ny * tb);
+  }
   if (c.case_id == 7) a.push_back(5LL * c.nghost * c.ny * c.nz * 8);
   if (c.case_id == 8) a.push_back(5LL * c.nghost * 8);
   if (c.case_id == 5) a.push_back((long long)(c.nx + 2 * c.nghost + 1) * 8);
@@ -828,9 +832,24 @@ int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m) {
     if (!h->face[d] && (rc = dalloc(h, &h->face[d], T[d].size()))) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(h->face[d], T[d].data(), T[d].size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   }
+  std::vector<float> Cf, Tf[3];
+  if (h->mixed) {  // FP32 copies for the FP32 arithmetic of the mixed policy
+    Cf.assign(C.begin(), C.end());
+    if (!h->centre_f && (rc = dalloc(h, &h->centre_f, Cf.size()))) return rc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->centre_f, Cf.data(), Cf.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    for (int d = 0; d < 3; ++d) {
+      if (T[d].empty()) continue;
+      Tf[d].assign(T[d].begin(), T[d].end());
+      if (!h->face_f[d] && (rc = dalloc(h, &h->face_f[d], Tf[d].size()))) return rc;
+      CUDA_TRY(h, cudaMemcpyAsync(h->face_f[d], Tf[d].data(), Tf[d].size() * sizeof(float), cudaMemcpyHostToDevice,
+                                  h->stream));
+    }
+  }
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));  // host vectors go out of scope
   h->G.centre = h->centre;
   for (int d = 0; d < 3; ++d) h->G.face[d] = h->face[d];
+  h->G.centre_f = h->centre_f;
+  for (int d = 0; d < 3; ++d) h->G.face_f[d] = h->face_f[d];
   h->metric_set = true;
   h->dt_valid = false;
   ++h->version;
@@ -1243,7 +1262,8 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
     delete h->self;
   }
   void *bufs[] = {h->G.P, h->G.U, h->G.UP, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1], h->G.F[2], h->G.cnt, h->G.clock,
-                  h->centre, h->face[0], h->face[1], h->face[2], h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],
+                  h->centre, h->face[0], h->face[1], h->face[2], h->centre_f, h->face_f[0], h->face_f[1], h->face_f[2],
+                  h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],
                   h->frozen[2], h->red, h->staging};
   for (void *b : bufs) if (b) cudaFree(b);
   if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);

@@ -137,6 +137,10 @@ struct GridDev {
   long long nij;
   const double *face[3];  // [NFF][nface_d]
   long long nface[3];
+  // FP32 copies of the tables for the mixed policy's FP32 arithmetic (sources, Riemann
+  // solver): the same values rounded once at upload instead of at every load; NULL for FP64
+  const float *centre_f;
+  const float *face_f[3];
   // boundary data
   const double *inj;     // Michel injector [v][g][j][k]  (5*g*ny*nz)
   const double *dust;    // [v][g]
@@ -155,6 +159,14 @@ struct GridDev {
   unsigned long long *cnt;      // failure / floor counters
   GridClock *clock;             // device clock of the grid
 };
+
+// the table of the arithmetic type R (double: the FP64 tables; float: their FP32 copies)
+template <class R> __device__ __forceinline__ const R *centre_table(const GridDev &G);
+template <> __device__ __forceinline__ const double *centre_table<double>(const GridDev &G) { return G.centre; }
+template <> __device__ __forceinline__ const float *centre_table<float>(const GridDev &G) { return G.centre_f; }
+template <class R> __device__ __forceinline__ const R *face_table(const GridDev &G, int d);
+template <> __device__ __forceinline__ const double *face_table<double>(const GridDev &G, int d) { return G.face[d]; }
+template <> __device__ __forceinline__ const float *face_table<float>(const GridDev &G, int d) { return G.face_f[d]; }
 
 // one block of a batched launch: the grid it works on and its first item (face or cell)
 struct BlockMap {
