@@ -894,7 +894,7 @@ int grhd2_gpu_set_bc_data(grhd2_gpu *h, const grhd2_gpu_bc_view *b) {
   return GRHD2_OK;
 }
 
-int grhd2_gpu_upload(grhd2_gpu *h, const double *up, const double *p) {
+static int upload_impl(grhd2_gpu *h, const double *up, const double *p, bool sync) {
   if (!h) return GRHD2_ERR_ARG;
   CUDA_TRY(h, cudaSetDevice(h->device));
   const GridDev &G = h->G;
@@ -915,9 +915,12 @@ int grhd2_gpu_upload(grhd2_gpu *h, const double *up, const double *p) {
     if (int rc = launch_check(h)) return rc;
     h->cons_set = true;
   }
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (sync) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return GRHD2_OK;
 }
+
+int grhd2_gpu_upload(grhd2_gpu *h, const double *up, const double *p) { return upload_impl(h, up, p, true); }
+int grhd2_gpu_upload_async(grhd2_gpu *h, const double *up, const double *p) { return upload_impl(h, up, p, false); }
 
 int grhd2_gpu_prim_to_cons_all(grhd2_gpu *h) {
   if (int rc = ready(h, false)) return rc;
@@ -1041,7 +1044,7 @@ int grhd2_gpu_set_boundary(grhd2_gpu *h) {
   return GRHD2_OK;
 }
 
-int grhd2_gpu_download(grhd2_gpu *h, double *up, double *p) {
+static int download_impl(grhd2_gpu *h, double *up, double *p, bool sync) {
   if (int rc = ready(h, false)) return rc;
   const GridDev &G = h->G;
   if (p) {
@@ -1059,9 +1062,12 @@ int grhd2_gpu_download(grhd2_gpu *h, double *up, double *p) {
     if (int rc = launch_check(h)) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(up, h->staging, h->n_interior * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   }
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (sync) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return GRHD2_OK;
 }
+
+int grhd2_gpu_download(grhd2_gpu *h, double *up, double *p) { return download_impl(h, up, p, true); }
+int grhd2_gpu_download_async(grhd2_gpu *h, double *up, double *p) { return download_impl(h, up, p, false); }
 
 int grhd2_gpu_get_counters(grhd2_gpu *h, grhd2_gpu_counters *out) {
   if (!h || !out) return GRHD2_ERR_ARG;

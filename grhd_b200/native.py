@@ -82,6 +82,8 @@ GPU_SYMBOLS = {
     "grhd2_gpu_cons_to_prim_all": (C.c_int, [_VP]),
     "grhd2_gpu_set_boundary": (C.c_int, [_VP]),
     "grhd2_gpu_download": (C.c_int, [_VP, c_double_p, c_double_p]),
+    "grhd2_gpu_upload_async": (C.c_int, [_VP, c_double_p, c_double_p]),
+    "grhd2_gpu_download_async": (C.c_int, [_VP, c_double_p, c_double_p]),
     "grhd2_gpu_get_counters": (C.c_int, [_VP, C.POINTER(Counters)]),
     "grhd2_gpu_reset_counters": (C.c_int, [_VP]),
     "grhd2_gpu_riemann_faces": (C.c_int, [_VP, C.c_int, C.c_int, c_double_p, c_double_p,

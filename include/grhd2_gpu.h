@@ -134,6 +134,13 @@ int grhd2_gpu_set_boundary(grhd2_gpu *h);
  * set_boundary_conditions fills it; ghost cells outside in two or more directions
  * (never read by calc_rhs) are left untouched in the caller's array. */
 int grhd2_gpu_download(grhd2_gpu *h, double *up, double *p);
+/* Asynchronous upload / download (no reference counterpart): the same copies and layout
+ * conversions, enqueued on the handle's stream without waiting.  The host arrays must stay
+ * valid and unchanged until the stream has finished (grhd2_gpu_synchronize); page-locked
+ * host memory lets the copies overlap kernels of other streams.  A caller that moves the
+ * state every step pipelines its grids this way instead of waiting after each copy. */
+int grhd2_gpu_upload_async(grhd2_gpu *h, const double *up, const double *p);
+int grhd2_gpu_download_async(grhd2_gpu *h, double *up, double *p);
 int grhd2_gpu_get_counters(grhd2_gpu *h, grhd2_gpu_counters *out);
 int grhd2_gpu_reset_counters(grhd2_gpu *h);
 /* Face fluxes for n independent faces (resolve_riemann_problem, fluxes.f90:56):
