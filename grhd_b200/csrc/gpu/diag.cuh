@@ -1,0 +1,190 @@
+// diag.cuh -- diagnostics of the resident state as device reductions, so the state does
+// not leave the GPU at diagnostic strides:
+//   total mass        grhd2.f90:283-301   sum u(D) dx dy dz
+//   accretion rate    output.f90:951-992  -sum_{j,k} up(D) (alpha v^x - beta^x) dy dz at i = idx_probe
+//   PPI modes         output.f90:995-1049 per-k azimuthal mass of cells with rho > 1e3 rho_floor
+//                                         (the host forms the m = 1..4 Fourier sums)
+//   global diagnostics output.f90:1052-1125 masses, angular momentum, extrema, counts
+// Every per-cell term is evaluated with the reference's operation order; the sums are
+// reduced in a fixed tree (fixed block count, warp shuffles, one final block), so a result
+// is reproducible run to run, and differs from a serial sum only by summation order.
+#pragma once
+
+#include "state.cuh"
+
+namespace grhd {
+
+constexpr int DIAG_BS = 256;
+constexpr int DIAG_BLOCKS = 592;  // 4 x 148 SMs
+
+// sum over the block (deterministic tree); result valid in thread 0
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[DIAG_BS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < DIAG_BS / 32 ? ws[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+__device__ __forceinline__ double block_min(double v) {
+  __shared__ double ws[DIAG_BS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < DIAG_BS / 32 ? ws[lane] : DBL_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+  }
+  return v;
+}
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double ws[DIAG_BS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < DIAG_BS / 32 ? ws[lane] : -DBL_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  }
+  return v;
+}
+
+// partial results of the global diagnostics
+struct DiagGlobal {
+  double mass, disk, angmom, rho_min, p_min, rho_max, p_max, vsq_max;
+  double atmosphere, invalid;  // counts (exact in double below 2^53)
+};
+
+__device__ __forceinline__ DiagGlobal diag_reduce(DiagGlobal a) {
+  DiagGlobal r;
+  r.mass = block_sum(a.mass);
+  r.disk = block_sum(a.disk);
+  r.angmom = block_sum(a.angmom);
+  r.rho_min = block_min(a.rho_min);
+  r.p_min = block_min(a.p_min);
+  r.rho_max = block_max(a.rho_max);
+  r.p_max = block_max(a.p_max);
+  r.vsq_max = block_max(a.vsq_max);
+  r.atmosphere = block_sum(a.atmosphere);
+  r.invalid = block_sum(a.invalid);
+  return r;
+}
+
+// calc_global_diagnostics over the cells, grid-stride; one partial per block
+template <class PT>
+__global__ void __launch_bounds__(DIAG_BS) k_diag_global(const GridDev G, const PT *__restrict__ P,
+                                                         const double *__restrict__ UP, DiagGlobal *__restrict__ part) {
+  const double cell_volume = G.dx * G.dy * G.dz;
+  const double density_cut = 1.0e3 * G.rho_floor;
+  DiagGlobal a{0.0, 0.0, 0.0, DBL_MAX, DBL_MAX, -DBL_MAX, -DBL_MAX, 0.0, 0.0, 0.0};
+  for (long long c = (long long)blockIdx.x * DIAG_BS + threadIdx.x; c < G.ncell; c += (long long)gridDim.x * DIAG_BS) {
+    const long long ij = c % G.nij;
+    const double rho = (double)P[c], pres = (double)P[G.pplane + c];
+    const double v[3] = {(double)P[2 * G.pplane + c], (double)P[3 * G.pplane + c], (double)P[4 * G.pplane + c]};
+    const double *T = G.centre;
+    const long long S = G.nij;
+    const int gi[3][3] = {{CF_G11, CF_G12, CF_G13}, {CF_G12, CF_G22, CF_G23}, {CF_G13, CF_G23, CF_G33}};
+    double v_sq = 0.0;  // output.f90:1081-1086, loop order ii, jj
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj) v_sq = v_sq + T[gi[ii][jj] * S + ij] * v[ii] * v[jj];
+    if (!isfinite(rho) || !isfinite(pres) || !isfinite(v_sq) || rho <= 0.0 || pres <= 0.0 || v_sq < 0.0 ||
+        v_sq >= 1.0)
+      a.invalid += 1.0;
+    if (isfinite(rho)) { a.rho_min = fmin(a.rho_min, rho); a.rho_max = fmax(a.rho_max, rho); }
+    if (isfinite(pres)) { a.p_min = fmin(a.p_min, pres); a.p_max = fmax(a.p_max, pres); }
+    if (isfinite(v_sq)) a.vsq_max = fmax(a.vsq_max, v_sq);
+    const double D = UP[c];
+    a.mass += D * cell_volume;
+    a.angmom += UP[4 * G.pplane + c] * cell_volume;
+    if (rho > density_cut) a.disk += D * cell_volume;
+    else a.atmosphere += 1.0;
+  }
+  const DiagGlobal r = diag_reduce(a);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(DIAG_BS) k_diag_global_final(const DiagGlobal *__restrict__ part, int n,
+                                                               DiagGlobal *__restrict__ out) {
+  DiagGlobal a{0.0, 0.0, 0.0, DBL_MAX, DBL_MAX, -DBL_MAX, -DBL_MAX, 0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < n; b += DIAG_BS) {
+    const DiagGlobal p = part[b];
+    a.mass += p.mass; a.disk += p.disk; a.angmom += p.angmom;
+    a.rho_min = fmin(a.rho_min, p.rho_min); a.p_min = fmin(a.p_min, p.p_min);
+    a.rho_max = fmax(a.rho_max, p.rho_max); a.p_max = fmax(a.p_max, p.p_max);
+    a.vsq_max = fmax(a.vsq_max, p.vsq_max);
+    a.atmosphere += p.atmosphere; a.invalid += p.invalid;
+  }
+  const DiagGlobal r = diag_reduce(a);
+  if (threadIdx.x == 0) *out = r;
+}
+
+// sum of u(D) dx dy dz (grhd2.f90:296: total_mass + u(eq_de) * dx * dy * dz)
+__global__ void __launch_bounds__(DIAG_BS) k_diag_mass(const GridDev G, const double *__restrict__ U,
+                                                       double *__restrict__ part) {
+  double a = 0.0;
+  for (long long c = (long long)blockIdx.x * DIAG_BS + threadIdx.x; c < G.ncell; c += (long long)gridDim.x * DIAG_BS)
+    a += U[c] * G.dx * G.dy * G.dz;
+  const double r = block_sum(a);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(DIAG_BS) k_sum_final(const double *__restrict__ part, int n, double *__restrict__ out) {
+  double a = 0.0;
+  for (int b = threadIdx.x; b < n; b += DIAG_BS) a += part[b];
+  const double r = block_sum(a);
+  if (threadIdx.x == 0) *out = r;
+}
+
+// accretion rate through the shell of cells i = idx (0-based), one block
+template <class PT>
+__global__ void __launch_bounds__(DIAG_BS) k_diag_mdot(const GridDev G, const PT *__restrict__ P,
+                                                       const double *__restrict__ UP, int idx, double *__restrict__ out) {
+  double a = 0.0;
+  const long long n = (long long)G.ny * G.nz;
+  for (long long s = threadIdx.x; s < n; s += DIAG_BS) {
+    const long long j = s % G.ny, k = s / G.ny;
+    const long long c = idx + (long long)G.nx * (j + (long long)G.ny * k);
+    const long long ij = idx + (long long)G.nx * j;
+    const double alpha = G.centre[(long long)CF_ALPHA * G.nij + ij];
+    const double beta1 = G.centre[(long long)CF_B1 * G.nij + ij];
+    const double v_eff = alpha * (double)P[2 * G.pplane + c] - beta1;
+    a += UP[c] * v_eff * G.dy * G.dz;
+  }
+  const double r = block_sum(a);
+  if (threadIdx.x == 0) *out = -r;
+}
+
+// mass of the cells above the density cut in each k-plane (one block per k)
+template <class PT>
+__global__ void __launch_bounds__(DIAG_BS) k_diag_azimuthal(const GridDev G, const PT *__restrict__ P,
+                                                            const double *__restrict__ UP, double *__restrict__ out) {
+  const double cell_volume = G.dx * G.dy * G.dz;
+  const double density_cut = 1.0e3 * G.rho_floor;
+  const long long k = blockIdx.x;
+  double a = 0.0;
+  for (long long ij = threadIdx.x; ij < G.nij; ij += DIAG_BS) {
+    const long long c = ij + G.nij * k;
+    if ((double)P[c] > density_cut) a += UP[c] * cell_volume;
+  }
+  const double r = block_sum(a);
+  if (threadIdx.x == 0) out[k] = r;
+}
+
+}  // namespace grhd

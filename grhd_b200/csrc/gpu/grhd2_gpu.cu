@@ -32,6 +32,7 @@
 #include "grhd2_gpu.h"
 #include "flux_launch.h"
 #include "frame.h"
+#include "diag.cuh"
 #include "kernels.cuh"
 
 using namespace grhd;
@@ -131,6 +132,8 @@ struct grhd2_gpu {
   double *inj = nullptr, *dust = nullptr, *xc = nullptr, *frozen[3] = {nullptr, nullptr, nullptr};
   unsigned long long *red = nullptr;
   double *staging = nullptr;
+  char *diag = nullptr;  // diagnostics scratch: block partials, results, per-k sums
+  bool u_valid = false;  // u has been written by a step (the mass monitor sums u)
   size_t n_ghosted = 0, n_interior = 0;
   GridClock hclock{};  // host mirror of the device clock
   int version = 0;     // bumped whenever G changes (batches refresh their device copies)
@@ -486,6 +489,7 @@ int batch_steps(grhd2_gpu_batch *b, long long nsteps, bool use_graph) {
       return bfail(b, GRHD2_ERR_STATE, "grid %zu moved to another stream after the batch was created", g);
   if (int rc = refresh_batch(b)) return rc;
   if (nsteps <= 0) return 0;
+  for (auto *m : b->m) m->u_valid = true;
   if (b->persistent) return enqueue_persistent(b, nsteps);
   if (!use_graph) {
     for (long long s = 0; s < nsteps; ++s)
@@ -592,6 +596,11 @@ int profile_common(grhd2_gpu_batch *b, float *ms, const char **names, int cap, i
 
 }  // namespace
 
+// diagnostics scratch: DIAG_BLOCKS partials, one result, nz per-plane sums
+size_t diag_bytes(int nz) {
+  return (size_t)(DIAG_BLOCKS + 1) * sizeof(DiagGlobal) + (size_t)(DIAG_BLOCKS + 1 + nz) * sizeof(double);
+}
+
 // device bytes a handle of this configuration allocates (create + set_metric + set_bc_data;
 // the calc_rhs scratch is not counted), each allocation rounded up to 4 KB
 long long handle_bytes(const grhd2_gpu_config &c) {
@@ -613,6 +622,7 @@ long long handle_bytes(const grhd2_gpu_config &c) {
   a.push_back(NCNT * 8);
   a.push_back((long long)sizeof(GridClock));
   a.push_back(32);
+  a.push_back((long long)diag_bytes(c.nz));
   a.push_back(5LL * (c.nx + 2 * c.nghost + 1) * (c.ny + 2 * c.nghost + 1) * (c.nz + 2 * c.nghost + 1) * 8);
   if (c.nghost == 2) {
     a.push_back(5LL * c.ny * c.nz * 8);
@@ -747,6 +757,7 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   if ((rc = dalloc(h, &G.cnt, NCNT))) return rc;
   if ((rc = dalloc(h, &G.clock, 1))) return rc;
   if ((rc = dalloc(h, &h->red, 4))) return rc;
+  if ((rc = dalloc(h, &h->diag, diag_bytes(c.nz)))) return rc;
   CUDA_TRY(h, cudaMemsetAsync(G.cnt, 0, NCNT * sizeof(unsigned long long), h->stream));
   h->hclock = GridClock{0.0, 0.0, 0.0, 0.0, 0, -1, 0, 1};
   if ((rc = write_clock(h))) return rc;
@@ -1234,6 +1245,88 @@ int grhd2_gpu_riemann_faces_noalloc(grhd2_gpu *h, int n, int dir, const double *
   return GRHD2_OK;
 }
 
+// ---- diagnostics ------------------------------------------------------------------------
+int grhd2_gpu_total_mass(grhd2_gpu *h, double *out) {
+  if (!out) return fail(h, GRHD2_ERR_ARG, "out is NULL");
+  if (int rc = ready(h, true)) return rc;
+  if (!h->u_valid) return fail(h, GRHD2_ERR_STATE, "no step has run: the mass monitor sums u, the state at the start of the last step");
+  double *part = (double *)(h->diag + (DIAG_BLOCKS + 1) * sizeof(DiagGlobal));
+  k_diag_mass<<<DIAG_BLOCKS, DIAG_BS, 0, h->stream>>>(h->G, h->G.U, part);
+  k_sum_final<<<1, DIAG_BS, 0, h->stream>>>(part, DIAG_BLOCKS, part + DIAG_BLOCKS);
+  if (int rc = launch_check(h)) return rc;
+  CUDA_TRY(h, cudaMemcpyAsync(out, part + DIAG_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_mdot(grhd2_gpu *h, int idx_probe, double *out) {
+  if (!out) return fail(h, GRHD2_ERR_ARG, "out is NULL");
+  if (int rc = ready(h, true)) return rc;
+  if (idx_probe < 1 || idx_probe > h->cfg.nx)
+    return fail(h, GRHD2_ERR_ARG, "CRITICAL ERROR: invalid accretion-probe index: %d", idx_probe);
+  double *res = (double *)(h->diag + (DIAG_BLOCKS + 1) * sizeof(DiagGlobal));
+  if (h->mixed) k_diag_mdot<float><<<1, DIAG_BS, 0, h->stream>>>(h->G, (const float *)h->G.P, h->G.UP, idx_probe - 1, res);
+  else k_diag_mdot<double><<<1, DIAG_BS, 0, h->stream>>>(h->G, (const double *)h->G.P, h->G.UP, idx_probe - 1, res);
+  if (int rc = launch_check(h)) return rc;
+  CUDA_TRY(h, cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_ppi_modes(grhd2_gpu *h, const double *z, double *values) {
+  if (!z || !values) return fail(h, GRHD2_ERR_ARG, "z or values is NULL");
+  if (int rc = ready(h, true)) return rc;
+  const int nz = h->cfg.nz, MAXM = 4;
+  for (int q = 0; q < 1 + 4 * MAXM; ++q) values[q] = 0.0;
+  if (nz < 2) return GRHD2_OK;  // output.f90:1005: no azimuthal direction
+  double *plane = (double *)(h->diag + (DIAG_BLOCKS + 1) * sizeof(DiagGlobal)) + DIAG_BLOCKS + 1;
+  if (h->mixed) k_diag_azimuthal<float><<<nz, DIAG_BS, 0, h->stream>>>(h->G, (const float *)h->G.P, h->G.UP, plane);
+  else k_diag_azimuthal<double><<<nz, DIAG_BS, 0, h->stream>>>(h->G, (const double *)h->G.P, h->G.UP, plane);
+  if (int rc = launch_check(h)) return rc;
+  std::vector<double> am(nz);
+  CUDA_TRY(h, cudaMemcpyAsync(am.data(), plane, nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  // output.f90:1024-1047, on the host: nz terms per mode
+  double c0 = 0.0, cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+  for (int k = 0; k < nz; ++k) {
+    c0 = c0 + am[k];
+    for (int m = 1; m <= MAXM; ++m) {
+      cr[m - 1] = cr[m - 1] + am[k] * std::cos((double)m * z[k]);
+      ci[m - 1] = ci[m - 1] - am[k] * std::sin((double)m * z[k]);
+    }
+  }
+  values[0] = c0;
+  for (int m = 1; m <= MAXM; ++m) {
+    double *v = values + 1 + 4 * (m - 1);
+    v[0] = cr[m - 1];
+    v[1] = ci[m - 1];
+    if (c0 > DBL_MIN) {
+      v[2] = std::sqrt(cr[m - 1] * cr[m - 1] + ci[m - 1] * ci[m - 1]) / c0;
+      v[3] = -std::atan2(ci[m - 1], cr[m - 1]) / (double)m;
+    }
+  }
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_global_diagnostics(grhd2_gpu *h, grhd2_gpu_diagnostics *out) {
+  if (!out) return fail(h, GRHD2_ERR_ARG, "out is NULL");
+  if (int rc = ready(h, true)) return rc;
+  DiagGlobal *part = (DiagGlobal *)h->diag;
+  if (h->mixed) k_diag_global<float><<<DIAG_BLOCKS, DIAG_BS, 0, h->stream>>>(h->G, (const float *)h->G.P, h->G.UP, part);
+  else k_diag_global<double><<<DIAG_BLOCKS, DIAG_BS, 0, h->stream>>>(h->G, (const double *)h->G.P, h->G.UP, part);
+  k_diag_global_final<<<1, DIAG_BS, 0, h->stream>>>(part, DIAG_BLOCKS, part + DIAG_BLOCKS);
+  if (int rc = launch_check(h)) return rc;
+  DiagGlobal r;
+  CUDA_TRY(h, cudaMemcpyAsync(&r, part + DIAG_BLOCKS, sizeof r, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  out->mass_total = r.mass; out->disk_mass = r.disk; out->angular_momentum = r.angmom;
+  out->rho_min = r.rho_min; out->p_min = r.p_min; out->rho_max = r.rho_max; out->p_max = r.p_max;
+  out->max_v_sq = r.vsq_max;
+  out->atmosphere_cells = (int64_t)r.atmosphere;
+  out->invalid_cells = (int64_t)r.invalid;
+  return GRHD2_OK;
+}
+
 int grhd2_gpu_get_stream(grhd2_gpu *h, void **stream_out) {
   if (!h || !stream_out) return GRHD2_ERR_ARG;
   *stream_out = (void *)h->stream;
@@ -1270,7 +1363,7 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
   void *bufs[] = {h->G.P, h->G.U, h->G.UP, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1], h->G.F[2], h->G.cnt, h->G.clock,
                   h->centre, h->face[0], h->face[1], h->face[2], h->centre_f, h->face_f[0], h->face_f[1], h->face_f[2],
                   h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],
-                  h->frozen[2], h->red, h->staging};
+                  h->frozen[2], h->red, h->staging, h->diag};
   for (void *b : bufs) if (b) cudaFree(b);
   if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
   delete h;

@@ -56,6 +56,16 @@ class Counters(C.Structure):
         return {n: int(getattr(self, n)) for n in COUNTER_NAMES}
 
 
+class Diagnostics(C.Structure):
+    """grhd2_gpu_diagnostics (include/grhd2_gpu.h)."""
+    _fields_ = [(n, C.c_double) for n in ("mass_total", "disk_mass", "angular_momentum", "rho_min", "p_min",
+                                         "rho_max", "p_max", "max_v_sq")] + \
+        [(n, C.c_int64) for n in ("atmosphere_cells", "invalid_cells")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class ProblemInfo(C.Structure):
     """grhd2_problem_info (include/grhd2_host.h)."""
     _fields_ = [(n, C.c_int32) for n in ("case_id", "nx", "ny", "nz", "nghost",
@@ -83,6 +93,10 @@ GPU_SYMBOLS = {
     "grhd2_gpu_set_boundary": (C.c_int, [_VP]),
     "grhd2_gpu_download": (C.c_int, [_VP, c_double_p, c_double_p]),
     "grhd2_gpu_upload_async": (C.c_int, [_VP, c_double_p, c_double_p]),
+    "grhd2_gpu_global_diagnostics": (C.c_int, [_VP, C.POINTER(Diagnostics)]),
+    "grhd2_gpu_total_mass": (C.c_int, [_VP, c_double_p]),
+    "grhd2_gpu_mdot": (C.c_int, [_VP, C.c_int, c_double_p]),
+    "grhd2_gpu_ppi_modes": (C.c_int, [_VP, c_double_p, c_double_p]),
     "grhd2_gpu_download_async": (C.c_int, [_VP, c_double_p, c_double_p]),
     "grhd2_gpu_get_counters": (C.c_int, [_VP, C.POINTER(Counters)]),
     "grhd2_gpu_reset_counters": (C.c_int, [_VP]),

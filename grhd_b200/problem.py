@@ -110,6 +110,29 @@ class Problem:
         z = np.ctypeslib.as_array(lib.grhd2_problem_z(self._h), shape=(self.nz + 2 * g + 1,)).copy()
         return x, y, z
 
+    def accretion_probe(self) -> int:
+        """Index of the accretion probe (initialization.f90:146-161): the first cell whose
+        centre lies outside the horizon r_+ = M + sqrt(M^2 - a^2) (log r coordinate when the
+        grid is logarithmic); 1 when the horizon is below the grid, 0 when above it."""
+        import math
+        info = self.info
+        m, a = info.bh_mass, info.a_spin
+        r_h = m + math.sqrt(max(0.0, m * m - a * a))
+        if self.config(0).use_log_r:
+            r_h = math.log(r_h)
+        x, _, _ = self.coords()
+        g = self.ng
+        xc = x[g + 1:g + 1 + self.nx]
+        xf = np.ctypeslib.as_array(self.metric_view().x_face, shape=(self.nx + 1,))
+        if r_h < xf[0]:
+            return 1
+        if r_h > xf[self.nx]:
+            return 0
+        for i, xi in enumerate(xc, start=1):
+            if xi >= r_h:
+                return i
+        return 0
+
     def eval_metric(self, x: float, y: float) -> dict:
         out = {k: np.zeros(n) for k, n in (("beta", 3), ("gamma", 9), ("gmunu", 16),
                                             ("dlnalpha", 4), ("chris", 64), ("dg", 48))}

@@ -129,6 +129,33 @@ class GpuGrid:
         self._check(self.lib.grhd2_gpu_download(self._h, N.dptr(up), N.dptr(p)))
         return up, p
 
+    # ---- diagnostics (device reductions) -------------------------------------------
+    def global_diagnostics(self) -> dict:
+        """calc_global_diagnostics (output.f90:1052) of the resident state."""
+        d = N.Diagnostics()
+        self._check(self.lib.grhd2_gpu_global_diagnostics(self._h, C.byref(d)))
+        return d.as_dict()
+
+    def total_mass(self) -> float:
+        """The time loop's mass monitor (grhd2.f90:283-301): sum u(D) dx dy dz."""
+        out = C.c_double()
+        self._check(self.lib.grhd2_gpu_total_mass(self._h, C.byref(out)))
+        return out.value
+
+    def mdot(self, idx_probe: int | None = None) -> float:
+        """calc_m_dot (output.f90:951) at the probe cell (default: the problem's)."""
+        idx = self.problem.accretion_probe() if idx_probe is None else idx_probe
+        out = C.c_double()
+        self._check(self.lib.grhd2_gpu_mdot(self._h, int(idx), C.byref(out)))
+        return out.value
+
+    def ppi_modes(self) -> np.ndarray:
+        """calc_ppi_modes (output.f90:995) values without the time column (17 numbers)."""
+        z = np.ascontiguousarray(self.problem.coords()[2][self.problem.ng + 1:self.problem.ng + 1 + self.problem.nz])
+        out = np.zeros(17)
+        self._check(self.lib.grhd2_gpu_ppi_modes(self._h, N.dptr(z), N.dptr(out)))
+        return out
+
     def counters(self) -> dict:
         c = N.Counters()
         self._check(self.lib.grhd2_gpu_get_counters(self._h, C.byref(c)))

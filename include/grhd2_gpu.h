@@ -134,6 +134,26 @@ int grhd2_gpu_set_boundary(grhd2_gpu *h);
  * set_boundary_conditions fills it; ghost cells outside in two or more directions
  * (never read by calc_rhs) are left untouched in the caller's array. */
 int grhd2_gpu_download(grhd2_gpu *h, double *up, double *p);
+/* ---- diagnostics of the resident state (device reductions; no download needed) ------
+ * Per-cell terms follow the reference's arithmetic; sums run in a fixed parallel order,
+ * reproducible run to run, equal to the reference's serial loops up to summation order. */
+typedef struct {
+  double mass_total, disk_mass, angular_momentum;         /* sums of up(D), up(S_3) x cell volume */
+  double rho_min, p_min, rho_max, p_max, max_v_sq;       /* over finite values */
+  int64_t atmosphere_cells, invalid_cells;
+} grhd2_gpu_diagnostics;
+/* calc_global_diagnostics (output.f90:1052-1125) without its file output. */
+int grhd2_gpu_global_diagnostics(grhd2_gpu *h, grhd2_gpu_diagnostics *out);
+/* The mass monitor of the time loop (grhd2.f90:283-301): sum of u(D) dx dy dz, u being
+ * the state at the start of the last step (GRHD2_ERR_STATE before the first step). */
+int grhd2_gpu_total_mass(grhd2_gpu *h, double *out);
+/* calc_m_dot (output.f90:951-992): accretion rate through the cells i = idx_probe
+ * (1-based, the first cell centre outside the horizon, initialization.f90:146-161). */
+int grhd2_gpu_mdot(grhd2_gpu *h, int idx_probe, double *out);
+/* calc_ppi_modes (output.f90:995-1049) without the time column: values[0] = c0, then for
+ * m = 1..4: c_real, c_imag, |c_m|/c0, phase at values[1 + 4 (m-1) ...]; z = z(1:nz) cell
+ * centres.  All zero when nz < 2. */
+int grhd2_gpu_ppi_modes(grhd2_gpu *h, const double *z, double *values);
 /* Asynchronous upload / download (no reference counterpart): the same copies and layout
  * conversions, enqueued on the handle's stream without waiting.  The host arrays must stay
  * valid and unchanged until the stream has finished (grhd2_gpu_synchronize); page-locked

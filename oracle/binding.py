@@ -73,6 +73,10 @@ def lib(libm_exp: bool = False):
             "orc_run": (C.c_int64, [P, M, _dp, _dp, C.c_double, C.c_double, C.c_int64, _dp, K]),
             "orc_num_threads": (C.c_int, []),
             "orc_exp": (C.c_double, [C.c_double]),
+            "orc_total_mass": (C.c_double, [P, _dp]),
+            "orc_mdot": (C.c_int, [P, M, _dp, _dp, C.c_int, _dp]),
+            "orc_ppi_modes": (None, [P, _dp, _dp, _dp, _dp]),
+            "orc_global_diagnostics": (None, [P, M, _dp, _dp, _dp, C.POINTER(C.c_int64)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -162,6 +166,32 @@ class OracleRun:
                              _p(rhs), dt, C.byref(self.counters))
         if rc != 0:
             raise RuntimeError(f"oracle step error {rc}")
+
+    # diagnostics: grhd2.f90:283-301, output.f90:951-1125 (serial loops)
+    def total_mass(self, u: np.ndarray) -> float:
+        return float(self.L.orc_total_mass(C.byref(self.cfg), _p(np.ascontiguousarray(u))))
+
+    def mdot(self, idx_probe: int) -> float:
+        out = C.c_double()
+        rc = self.L.orc_mdot(C.byref(self.cfg), C.byref(self.met), _p(self.up), _p(self.p), idx_probe, C.byref(out))
+        if rc != 0:
+            raise ValueError("invalid accretion-probe index")
+        return out.value
+
+    def ppi_modes(self, z: np.ndarray) -> np.ndarray:
+        out = np.zeros(17)
+        self.L.orc_ppi_modes(C.byref(self.cfg), _p(self.up), _p(self.p), _p(np.ascontiguousarray(z)), _p(out))
+        return out
+
+    def global_diagnostics(self) -> dict:
+        f = np.zeros(8)
+        n = np.zeros(2, dtype=np.int64)
+        self.L.orc_global_diagnostics(C.byref(self.cfg), C.byref(self.met), _p(self.up), _p(self.p), _p(f),
+                                      n.ctypes.data_as(C.POINTER(C.c_int64)))
+        keys = ("mass_total", "disk_mass", "angular_momentum", "rho_min", "p_min", "rho_max", "p_max", "max_v_sq")
+        out = dict(zip(keys, f.tolist()))
+        out.update(atmosphere_cells=int(n[0]), invalid_cells=int(n[1]))
+        return out
 
     def run(self, t0: float, final_time: float, max_steps: int = -1):
         t = C.c_double()

@@ -1426,3 +1426,103 @@ int64_t orc_run(const orc_config *c, const orc_metric *m, double *up, double *p,
   if (t_out) *t_out = t;
   return rc ? (int64_t)rc : steps;
 }
+
+
+/* ------------------------------------------------------------------------------------
+ * Diagnostics: grhd2.f90:283-301 and output.f90:951-1125
+ * ------------------------------------------------------------------------------------ */
+double orc_total_mass(const orc_config *c, const double *u) {
+  double total = 0.0;
+  for (int k = 1; k <= c->nz; ++k)
+    for (int j = 1; j <= c->ny; ++j)
+      for (int i = 1; i <= c->nx; ++i) total = total + u[uidx(c, 0, i, j, k)] * c->dx * c->dy * c->dz;
+  return total;
+}
+
+int orc_mdot(const orc_config *c, const orc_metric *m, const double *up, const double *p, int idx_probe,
+             double *out) {
+  if (idx_probe < 1 || idx_probe > c->nx) return -1; /* output.f90:959-962 */
+  const lay_t L = mklay(c);
+  double m_dot = 0.0;
+  for (int k = 1; k <= c->nz; ++k)
+    for (int j = 1; j <= c->ny; ++j) {
+      const size_t q = cell(c, idx_probe, j);
+      const double alpha = m->alpha_c[q];
+      const double beta1 = m->beta_c[3 * q];
+      const double v_eff = alpha * p[pidx(&L, 2, idx_probe, j, k)] - beta1;
+      m_dot = m_dot + up[uidx(c, 0, idx_probe, j, k)] * v_eff * c->dy * c->dz;
+    }
+  *out = -m_dot;
+  return 0;
+}
+
+void orc_ppi_modes(const orc_config *c, const double *up, const double *p, const double *z, double *values) {
+  enum { MAXM = 4 };
+  const lay_t L = mklay(c);
+  for (int q = 0; q < 1 + 4 * MAXM; ++q) values[q] = 0.0;
+  if (c->nz < 2) return; /* output.f90:1005 */
+  const double cell_volume = c->dx * c->dy * c->dz;
+  const double density_cut = 1.0e3 * c->rho_floor;
+  double c0 = 0.0, cr[MAXM] = {0, 0, 0, 0}, ci[MAXM] = {0, 0, 0, 0};
+  for (int k = 1; k <= c->nz; ++k) {
+    double am = 0.0;
+    for (int j = 1; j <= c->ny; ++j)
+      for (int i = 1; i <= c->nx; ++i)
+        if (p[pidx(&L, 0, i, j, k)] > density_cut) am = am + up[uidx(c, 0, i, j, k)] * cell_volume;
+    c0 = c0 + am;
+    for (int mm = 1; mm <= MAXM; ++mm) {
+      cr[mm - 1] = cr[mm - 1] + am * cos((double)mm * z[k - 1]);
+      ci[mm - 1] = ci[mm - 1] - am * sin((double)mm * z[k - 1]);
+    }
+  }
+  values[0] = c0;
+  for (int mm = 1; mm <= MAXM; ++mm) {
+    double *v = values + 1 + 4 * (mm - 1);
+    v[0] = cr[mm - 1];
+    v[1] = ci[mm - 1];
+    if (c0 > DBL_MIN) {
+      v[2] = sqrt(cr[mm - 1] * cr[mm - 1] + ci[mm - 1] * ci[mm - 1]) / c0;
+      v[3] = -atan2(ci[mm - 1], cr[mm - 1]) / (double)mm;
+    }
+  }
+}
+
+void orc_global_diagnostics(const orc_config *c, const orc_metric *m, const double *up, const double *p,
+                            double *f, int64_t *n) {
+  const lay_t L = mklay(c);
+  const double cell_volume = c->dx * c->dy * c->dz;
+  const double density_cut = 1.0e3 * c->rho_floor;
+  double mass_total = 0.0, disk_mass = 0.0, angmom = 0.0;
+  double rmin = DBL_MAX, pmin = DBL_MAX, rmax_ = -DBL_MAX, pmax = -DBL_MAX, vmax = 0.0;
+  int64_t atmosphere = 0, invalid = 0;
+  for (int k = 1; k <= c->nz; ++k)
+    for (int j = 1; j <= c->ny; ++j)
+      for (int i = 1; i <= c->nx; ++i) {
+        const double rho = p[pidx(&L, 0, i, j, k)];
+        const double pres = p[pidx(&L, 1, i, j, k)];
+        const double *g = &m->gamma_c[9 * cell(c, i, j)];
+        double v_sq = 0.0;
+        for (int ii = 1; ii <= 3; ++ii)
+          for (int jj = 1; jj <= 3; ++jj)
+            v_sq = v_sq + G3(g, ii, jj) * p[pidx(&L, 1 + ii, i, j, k)] * p[pidx(&L, 1 + jj, i, j, k)];
+        if (!isfinite(rho) || !isfinite(pres) || !isfinite(v_sq) || rho <= 0.0 || pres <= 0.0 || v_sq < 0.0 ||
+            v_sq >= 1.0)
+          invalid++;
+        if (isfinite(rho)) {
+          if (rho < rmin) rmin = rho;
+          if (rho > rmax_) rmax_ = rho;
+        }
+        if (isfinite(pres)) {
+          if (pres < pmin) pmin = pres;
+          if (pres > pmax) pmax = pres;
+        }
+        if (isfinite(v_sq) && v_sq > vmax) vmax = v_sq;
+        mass_total = mass_total + up[uidx(c, 0, i, j, k)] * cell_volume;
+        angmom = angmom + up[uidx(c, 4, i, j, k)] * cell_volume;
+        if (rho > density_cut) disk_mass = disk_mass + up[uidx(c, 0, i, j, k)] * cell_volume;
+        else atmosphere++;
+      }
+  f[0] = mass_total; f[1] = disk_mass; f[2] = angmom;
+  f[3] = rmin; f[4] = pmin; f[5] = rmax_; f[6] = pmax; f[7] = vmax;
+  n[0] = atmosphere; n[1] = invalid;
+}

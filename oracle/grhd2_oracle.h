@@ -104,6 +104,21 @@ int orc_step(const orc_config *c, const orc_metric *m, double *u, double *up, do
 int64_t orc_run(const orc_config *c, const orc_metric *m, double *up, double *p,
                 double t0, double final_time, int64_t max_steps, double *t_out,
                 orc_counters *cnt);
+/* Diagnostics (loops in the reference's order, serial).
+ * grhd2.f90:283-301 mass monitor: sum of u(D) dx dy dz over interior cells */
+double orc_total_mass(const orc_config *c, const double *u);
+/* output.f90:951-992 calc_m_dot at cell i = idx_probe (1-based): -sum_j,k up(D) v_eff dy dz,
+ * v_eff = alpha p(vx) - beta^1; returns 0 and writes *out, or -1 for an invalid index */
+int orc_mdot(const orc_config *c, const orc_metric *m, const double *up, const double *p, int idx_probe,
+             double *out);
+/* output.f90:995-1049 calc_ppi_modes without the time column: values[0] = c0, then per
+ * mode m = 1..4: c_real, c_imag, |c|/c0, phase (values[1 + 4 (m-1) ..]); z = z(1:nz) */
+void orc_ppi_modes(const orc_config *c, const double *up, const double *p, const double *z, double *values);
+/* output.f90:1052-1125 calc_global_diagnostics without the time column:
+ * f = mass_total, disk_mass, angular_momentum, rho_min, p_min, rho_max, p_max, max_v_sq;
+ * n = atmosphere_cells, invalid_cells */
+void orc_global_diagnostics(const orc_config *c, const orc_metric *m, const double *up, const double *p,
+                            double *f, int64_t *n);
 /* number of OpenMP threads used by orc_run / orc_step (1 without OpenMP) */
 int orc_num_threads(void);
 /* the exp used by WENO3 (reconstruction.f90:169), exposed for its accuracy test */
