@@ -133,6 +133,11 @@ struct grhd2_gpu {
   unsigned long long *red = nullptr;
   double *staging = nullptr;
   char *diag = nullptr;  // diagnostics scratch: block partials, results, per-k sums
+  // checkpoint snapshot: up in the reference layout, copied out on its own stream
+  double *snap = nullptr;
+  cudaStream_t snap_stream = nullptr;
+  cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
+  bool snap_pending = false;
   bool u_valid = false;  // u has been written by a step (the mass monitor sums u)
   size_t n_ghosted = 0, n_interior = 0;
   GridClock hclock{};  // host mirror of the device clock
@@ -1327,6 +1332,39 @@ int grhd2_gpu_global_diagnostics(grhd2_gpu *h, grhd2_gpu_diagnostics *out) {
   return GRHD2_OK;
 }
 
+// ---- checkpoint snapshots ---------------------------------------------------------------
+int grhd2_gpu_snapshot_begin(grhd2_gpu *h, double *up_host) {
+  if (!up_host) return fail(h, GRHD2_ERR_ARG, "up_host is NULL");
+  if (int rc = ready(h, true)) return rc;
+  int rc;
+  if (!h->snap) {
+    if ((rc = dalloc(h, &h->snap, h->n_interior))) return rc;
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->snap_taken, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+  }
+  // the previous snapshot's copy must have left the buffer before it is overwritten
+  if (h->snap_pending) CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->snap_done, 0));
+  k_cons_out<<<nblocks(h->G.ncell, 256), 256, 0, h->stream>>>(h->G, h->G.UP, h->snap);
+  if ((rc = launch_check(h))) return rc;
+  CUDA_TRY(h, cudaEventRecord(h->snap_taken, h->stream));
+  CUDA_TRY(h, cudaStreamWaitEvent(h->snap_stream, h->snap_taken, 0));
+  CUDA_TRY(h, cudaMemcpyAsync(up_host, h->snap, h->n_interior * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->snap_stream));
+  CUDA_TRY(h, cudaEventRecord(h->snap_done, h->snap_stream));
+  h->snap_pending = true;
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_snapshot_wait(grhd2_gpu *h) {
+  if (!h) return GRHD2_ERR_ARG;
+  if (!h->snap_pending) return GRHD2_OK;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  CUDA_TRY(h, cudaEventSynchronize(h->snap_done));
+  h->snap_pending = false;
+  return GRHD2_OK;
+}
+
 int grhd2_gpu_get_stream(grhd2_gpu *h, void **stream_out) {
   if (!h || !stream_out) return GRHD2_ERR_ARG;
   *stream_out = (void *)h->stream;
@@ -1360,6 +1398,13 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
     destroy_batch_resources(h->self);
     delete h->self;
   }
+  if (h->snap_stream) {
+    cudaStreamSynchronize(h->snap_stream);
+    cudaStreamDestroy(h->snap_stream);
+  }
+  if (h->snap_taken) cudaEventDestroy(h->snap_taken);
+  if (h->snap_done) cudaEventDestroy(h->snap_done);
+  if (h->snap) cudaFree(h->snap);
   void *bufs[] = {h->G.P, h->G.U, h->G.UP, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1], h->G.F[2], h->G.cnt, h->G.clock,
                   h->centre, h->face[0], h->face[1], h->face[2], h->centre_f, h->face_f[0], h->face_f[1], h->face_f[2],
                   h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],

@@ -154,6 +154,15 @@ int grhd2_gpu_mdot(grhd2_gpu *h, int idx_probe, double *out);
  * m = 1..4: c_real, c_imag, |c_m|/c0, phase at values[1 + 4 (m-1) ...]; z = z(1:nz) cell
  * centres.  All zero when nz < 2. */
 int grhd2_gpu_ppi_modes(grhd2_gpu *h, const double *z, double *values);
+/* Checkpoint snapshot (feeds save_checkpoint, output.f90:475-531, which writes up):
+ * begin converts up to the reference layout in a device buffer on the handle's stream and
+ * copies it to up_host on a separate copy stream, returning at once; steps enqueued
+ * afterwards run while the copy proceeds.  wait blocks until up_host holds the snapshot;
+ * write the checkpoint file after it.  up_host must stay valid and untouched until then;
+ * page-locked memory lets the copy overlap the steps (pageable memory makes begin wait for
+ * the copy).  A new begin waits on the device for the previous copy. */
+int grhd2_gpu_snapshot_begin(grhd2_gpu *h, double *up_host);
+int grhd2_gpu_snapshot_wait(grhd2_gpu *h);
 /* Asynchronous upload / download (no reference counterpart): the same copies and layout
  * conversions, enqueued on the handle's stream without waiting.  The host arrays must stay
  * valid and unchanged until the stream has finished (grhd2_gpu_synchronize); page-locked
