@@ -187,4 +187,32 @@ __global__ void __launch_bounds__(DIAG_BS) k_diag_azimuthal(const GridDev G, con
   if (threadIdx.x == 0) out[k] = r;
 }
 
+// write_vtk_cell_data (output.f90:398-453): the 7 cell fields of a VTK frame exactly as
+// the file holds them -- rho, p, v^r (x r_scale on log-r grids), v^theta, v^phi, the lapse,
+// beta^r (x r_scale) -- each nx*ny*nz doubles in i-fastest order, big-endian.
+__device__ __forceinline__ unsigned long long bswap64(unsigned long long x) {
+  const unsigned lo = (unsigned)x, hi = (unsigned)(x >> 32);
+  const unsigned slo = __byte_perm(lo, 0, 0x0123), shi = __byte_perm(hi, 0, 0x0123);
+  return ((unsigned long long)slo << 32) | shi;
+}
+template <class PT>
+__global__ void __launch_bounds__(DIAG_BS) k_vtk_cells(const GridDev G, const PT *__restrict__ P,
+                                                       const double *__restrict__ r_scale,
+                                                       unsigned long long *__restrict__ out) {
+  for (long long c = (long long)blockIdx.x * DIAG_BS + threadIdx.x; c < G.ncell; c += (long long)gridDim.x * DIAG_BS) {
+    const long long ij = c % G.nij, i = ij % G.nx;
+    double f[7];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) f[v] = (double)P[v * G.pplane + c];
+    f[5] = G.centre[(long long)CF_ALPHA * G.nij + ij];
+    f[6] = G.centre[(long long)CF_B1 * G.nij + ij];
+    if (r_scale) {
+      f[2] = f[2] * r_scale[i];
+      f[6] = f[6] * r_scale[i];
+    }
+#pragma unroll
+    for (int q = 0; q < 7; ++q) out[q * G.ncell + c] = bswap64(__double_as_longlong(f[q]));
+  }
+}
+
 }  // namespace grhd

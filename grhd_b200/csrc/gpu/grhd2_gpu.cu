@@ -133,6 +133,7 @@ struct grhd2_gpu {
   unsigned long long *red = nullptr;
   double *staging = nullptr;
   char *diag = nullptr;  // diagnostics scratch: block partials, results, per-k sums
+  double *vtk = nullptr;  // VTK cell fields (big-endian) and radial scale factors
   // checkpoint snapshot: up in the reference layout, copied out on its own stream
   double *snap = nullptr;
   cudaStream_t snap_stream = nullptr;
@@ -1332,6 +1333,29 @@ int grhd2_gpu_global_diagnostics(grhd2_gpu *h, grhd2_gpu_diagnostics *out) {
   return GRHD2_OK;
 }
 
+// ---- VTK cell data ------------------------------------------------------------------------
+int grhd2_gpu_vtk_cell_data(grhd2_gpu *h, const double *r_scale, void *out_host) {
+  if (!out_host) return fail(h, GRHD2_ERR_ARG, "out_host is NULL");
+  if (int rc = ready(h, true)) return rc;
+  const size_t field = (size_t)h->G.ncell * sizeof(double);
+  int rc;
+  if (!h->vtk) {  // 7 fields, device scratch kept for later frames
+    if ((rc = dalloc(h, &h->vtk, 7 * (size_t)h->G.ncell + (size_t)h->cfg.nx))) return rc;
+  }
+  double *scale = nullptr;
+  if (r_scale) {
+    scale = h->vtk + 7 * (size_t)h->G.ncell;
+    CUDA_TRY(h, cudaMemcpyAsync(scale, r_scale, h->cfg.nx * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  }
+  unsigned long long *out = (unsigned long long *)h->vtk;
+  if (h->mixed) k_vtk_cells<float><<<DIAG_BLOCKS, DIAG_BS, 0, h->stream>>>(h->G, (const float *)h->G.P, scale, out);
+  else k_vtk_cells<double><<<DIAG_BLOCKS, DIAG_BS, 0, h->stream>>>(h->G, (const double *)h->G.P, scale, out);
+  if ((rc = launch_check(h))) return rc;
+  CUDA_TRY(h, cudaMemcpyAsync(out_host, out, 7 * field, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return GRHD2_OK;
+}
+
 // ---- checkpoint snapshots ---------------------------------------------------------------
 int grhd2_gpu_snapshot_begin(grhd2_gpu *h, double *up_host) {
   if (!up_host) return fail(h, GRHD2_ERR_ARG, "up_host is NULL");
@@ -1405,6 +1429,7 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
   if (h->snap_taken) cudaEventDestroy(h->snap_taken);
   if (h->snap_done) cudaEventDestroy(h->snap_done);
   if (h->snap) cudaFree(h->snap);
+  if (h->vtk) cudaFree(h->vtk);
   void *bufs[] = {h->G.P, h->G.U, h->G.UP, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1], h->G.F[2], h->G.cnt, h->G.clock,
                   h->centre, h->face[0], h->face[1], h->face[2], h->centre_f, h->face_f[0], h->face_f[1], h->face_f[2],
                   h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],

@@ -10,6 +10,7 @@ the library's message).  There is no CPU fallback: a missing library or device r
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -154,6 +155,18 @@ class GpuGrid:
         z = np.ascontiguousarray(self.problem.coords()[2][self.problem.ng + 1:self.problem.ng + 1 + self.problem.nz])
         out = np.zeros(17)
         self._check(self.lib.grhd2_gpu_ppi_modes(self._h, N.dptr(z), N.dptr(out)))
+        return out
+
+    def vtk_cell_data(self) -> np.ndarray:
+        """The 7 big-endian cell fields of a VTK frame (output.f90:398-453), shape
+        (7, nz, ny, nx), dtype '>f8'; v^r and beta^r scaled by exp(x) on log-r grids."""
+        pb = self.problem
+        r_scale = None
+        if self.cfg.use_log_r:
+            x = pb.coords()[0][pb.ng + 1:pb.ng + 1 + pb.nx]
+            r_scale = np.array([math.exp(v) for v in x])  # the C library's exp, as the reference's writer
+        out = np.empty((7, pb.nz, pb.ny, pb.nx), dtype=">f8")
+        self._check(self.lib.grhd2_gpu_vtk_cell_data(self._h, N.dptr(r_scale), out.ctypes.data_as(C.c_void_p)))
         return out
 
     def counters(self) -> dict:

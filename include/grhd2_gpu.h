@@ -154,6 +154,12 @@ int grhd2_gpu_mdot(grhd2_gpu *h, int idx_probe, double *out);
  * m = 1..4: c_real, c_imag, |c_m|/c0, phase at values[1 + 4 (m-1) ...]; z = z(1:nz) cell
  * centres.  All zero when nz < 2. */
 int grhd2_gpu_ppi_modes(grhd2_gpu *h, const double *z, double *values);
+/* The cell data of a VTK frame (write_vtk_cell_data, output.f90:398-453) as the file holds
+ * it: 7 blocks of nx*ny*nz big-endian doubles (i fastest) -- rho, p, v^1, v^2, v^3, alpha,
+ * beta^1 -- with v^1 and beta^1 multiplied by r_scale[i-1] = exp(x(i)) when r_scale is not
+ * NULL (the log-r grids; pass the host's exp values so the products equal a host writer's).
+ * The caller writes the headers and these bytes between them.  out_host: 56*nx*ny*nz bytes. */
+int grhd2_gpu_vtk_cell_data(grhd2_gpu *h, const double *r_scale, void *out_host);
 /* Checkpoint snapshot (feeds save_checkpoint, output.f90:475-531, which writes up):
  * begin converts up to the reference layout in a device buffer on the handle's stream and
  * copies it to up_host on a separate copy stream, returning at once; steps enqueued
