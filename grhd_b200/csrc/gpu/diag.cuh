@@ -187,6 +187,73 @@ __global__ void __launch_bounds__(DIAG_BS) k_diag_azimuthal(const GridDev G, con
   if (threadIdx.x == 0) out[k] = r;
 }
 
+// calc_gw_strain (output.f90:852-948): Finn-Evans stresses of the cells outside the horizon
+// with the numerical atmosphere subtracted.  tab = r(nx) | sin th, cos th (ny) | sin ph,
+// cos ph (nz), evaluated on the host with the C library so every per-cell term equals the
+// reference's.  One partial (Ixx, Iyy, Ixy) per block.
+template <class PT>
+__global__ void __launch_bounds__(DIAG_BS) k_diag_gw(const GridDev G, const PT *__restrict__ P,
+                                                     const double *__restrict__ tab, int use_log_r, double r_h,
+                                                     double bh_mass, double spin, double *__restrict__ part) {
+  const double *rr = tab, *sth = tab + G.nx, *cth = sth + G.ny, *sph = cth + G.ny, *cph = sph + G.nz;
+  double ixx = 0.0, iyy = 0.0, ixy = 0.0;
+  for (long long c = (long long)blockIdx.x * DIAG_BS + threadIdx.x; c < G.ncell; c += (long long)gridDim.x * DIAG_BS) {
+    const long long ij = c % G.nij, i = ij % G.nx, j = ij / G.nx, k = c / G.nij;
+    const double r = rr[i];
+    if (r <= r_h) continue;
+    double rho = (double)P[c] - G.rho_floor, pres = (double)P[G.pplane + c] - G.p_floor;
+    if (!(rho > 0.0)) rho = 0.0;
+    if (!(pres > 0.0)) pres = 0.0;
+    if (rho <= 0.0 && pres <= 0.0) continue;
+    const double alpha = G.centre[(long long)CF_ALPHA * G.nij + ij];
+    double rates[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      rates[d] = alpha * (double)P[(2 + d) * G.pplane + c] - G.centre[(long long)(CF_B1 + d) * G.nij + ij];
+    if (use_log_r) rates[0] = r * rates[0];
+    const double st = sth[j], ct = cth[j], sp = sph[k], cp = cph[k];
+    double pos[3], vel[3];
+    if (fabs(st) <= 64.0 * DBL_EPSILON) {
+      pos[0] = 0.0; pos[1] = 0.0; pos[2] = copysign(fabs(r), ct);
+    } else {
+      pos[0] = (r * cp - spin * sp) * st;
+      pos[1] = (r * sp + spin * cp) * st;
+      pos[2] = r * ct;
+    }
+    vel[0] = rates[0] * cp * st + rates[1] * (r * cp - spin * sp) * ct - rates[2] * (r * sp + spin * cp) * st;
+    vel[1] = rates[0] * sp * st + rates[1] * (r * sp + spin * cp) * ct + rates[2] * (r * cp - spin * sp) * st;
+    vel[2] = rates[0] * ct - r * rates[1] * st;
+    const double sigma = r * r + spin * spin * (ct * ct);
+    const double jac = sigma * st;
+    const double dV = jac * (use_log_r ? r : 1.0) * G.dx * G.dy * G.dz;
+    const double r2 = pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2];
+    const double mr3 = bh_mass / (r2 * sqrt(r2));
+    ixx += (2.0 * rho * (vel[0] * vel[0]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[0] * pos[0])) * dV;
+    iyy += (2.0 * rho * (vel[1] * vel[1]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[1] * pos[1])) * dV;
+    ixy += (2.0 * rho * vel[0] * vel[1] - 2.0 * rho * mr3 * pos[0] * pos[1]) * dV;
+  }
+  ixx = block_sum(ixx);
+  iyy = block_sum(iyy);
+  ixy = block_sum(ixy);
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = ixx;
+    part[3 * blockIdx.x + 1] = iyy;
+    part[3 * blockIdx.x + 2] = ixy;
+  }
+}
+
+__global__ void __launch_bounds__(DIAG_BS) k_sum3_final(const double *__restrict__ part, int n, double *__restrict__ out) {
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < n; b += DIAG_BS)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) a[q] += part[3 * b + q];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const double r = block_sum(a[q]);
+    if (threadIdx.x == 0) out[q] = r;
+  }
+}
+
 // write_vtk_cell_data (output.f90:398-453): the 7 cell fields of a VTK frame exactly as
 // the file holds them -- rho, p, v^r (x r_scale on log-r grids), v^theta, v^phi, the lapse,
 // beta^r (x r_scale) -- each nx*ny*nz doubles in i-fastest order, big-endian.

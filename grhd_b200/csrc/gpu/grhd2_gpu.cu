@@ -603,8 +603,11 @@ int profile_common(grhd2_gpu_batch *b, float *ms, const char **names, int cap, i
 }  // namespace
 
 // diagnostics scratch: DIAG_BLOCKS partials, one result, nz per-plane sums
-size_t diag_bytes(int nz) {
-  return (size_t)(DIAG_BLOCKS + 1) * sizeof(DiagGlobal) + (size_t)(DIAG_BLOCKS + 1 + nz) * sizeof(double);
+// diagnostics scratch: DIAG_BLOCKS partials and one result (global), DIAG_BLOCKS + 1 sums,
+// nz per-plane sums, 3 (DIAG_BLOCKS + 1) quadrupole sums, coordinate tables nx + 2 ny + 2 nz
+size_t diag_bytes(int nx, int ny, int nz) {
+  return (size_t)(DIAG_BLOCKS + 1) * sizeof(DiagGlobal) +
+         (size_t)(DIAG_BLOCKS + 1 + nz + 3 * (DIAG_BLOCKS + 1) + nx + 2 * ny + 2 * nz) * sizeof(double);
 }
 
 // device bytes a handle of this configuration allocates (create + set_metric + set_bc_data;
@@ -628,7 +631,7 @@ long long handle_bytes(const grhd2_gpu_config &c) {
   a.push_back(NCNT * 8);
   a.push_back((long long)sizeof(GridClock));
   a.push_back(32);
-  a.push_back((long long)diag_bytes(c.nz));
+  a.push_back((long long)diag_bytes(c.nx, c.ny, c.nz));
   a.push_back(5LL * (c.nx + 2 * c.nghost + 1) * (c.ny + 2 * c.nghost + 1) * (c.nz + 2 * c.nghost + 1) * 8);
   if (c.nghost == 2) {
     a.push_back(5LL * c.ny * c.nz * 8);
@@ -763,7 +766,7 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   if ((rc = dalloc(h, &G.cnt, NCNT))) return rc;
   if ((rc = dalloc(h, &G.clock, 1))) return rc;
   if ((rc = dalloc(h, &h->red, 4))) return rc;
-  if ((rc = dalloc(h, &h->diag, diag_bytes(c.nz)))) return rc;
+  if ((rc = dalloc(h, &h->diag, diag_bytes(c.nx, c.ny, c.nz)))) return rc;
   CUDA_TRY(h, cudaMemsetAsync(G.cnt, 0, NCNT * sizeof(unsigned long long), h->stream));
   h->hclock = GridClock{0.0, 0.0, 0.0, 0.0, 0, -1, 0, 1};
   if ((rc = write_clock(h))) return rc;
@@ -1311,6 +1314,43 @@ int grhd2_gpu_ppi_modes(grhd2_gpu *h, const double *z, double *values) {
       v[3] = -std::atan2(ci[m - 1], cr[m - 1]) / (double)m;
     }
   }
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_gw_strain(grhd2_gpu *h, const double *x, const double *y, const double *z, int use_log_r,
+                        double bh_mass, double spin, double *out) {
+  if (!x || !y || !z || !out) return fail(h, GRHD2_ERR_ARG, "invalid arguments to grhd2_gpu_gw_strain");
+  if (int rc = ready(h, true)) return rc;
+  for (int q = 0; q < 5; ++q) out[q] = 0.0;
+  if (h->cfg.metric_kind == GRHD2_METRIC_MINKOWSKI || bh_mass < 0.1) return GRHD2_OK;  // output.f90:864
+  // event_horizon_radius (metrics.f90:66-87)
+  if (bh_mass < 0.0) return fail(h, GRHD2_ERR_ARG, "CRITICAL ERROR: black-hole mass must be non-negative.");
+  const double big = std::max(1.0, std::max(bh_mass * bh_mass, spin * spin));
+  const double disc = bh_mass * bh_mass - spin * spin;
+  if (disc < -64.0 * DBL_EPSILON * big) return fail(h, GRHD2_ERR_ARG, "CRITICAL ERROR: Kerr spin must satisfy |a| <= M.");
+  const double r_h = bh_mass + std::sqrt(disc > 0.0 ? disc : 0.0);
+  const int nx = h->cfg.nx, ny = h->cfg.ny, nz = h->cfg.nz;
+  std::vector<double> tab((size_t)nx + 2 * ny + 2 * nz);
+  for (int i = 0; i < nx; ++i) tab[i] = use_log_r ? std::exp(x[i]) : x[i];
+  for (int j = 0; j < ny; ++j) { tab[nx + j] = std::sin(y[j]); tab[nx + ny + j] = std::cos(y[j]); }
+  for (int k = 0; k < nz; ++k) { tab[nx + 2 * ny + k] = std::sin(z[k]); tab[nx + 2 * ny + nz + k] = std::cos(z[k]); }
+  double *base = (double *)(h->diag + (DIAG_BLOCKS + 1) * sizeof(DiagGlobal)) + DIAG_BLOCKS + 1 + nz;
+  double *part = base, *res = base + 3 * DIAG_BLOCKS, *dtab = base + 3 * (DIAG_BLOCKS + 1);
+  CUDA_TRY(h, cudaMemcpyAsync(dtab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (h->mixed)
+    k_diag_gw<float><<<DIAG_BLOCKS, DIAG_BS, 0, h->stream>>>(h->G, (const float *)h->G.P, dtab, use_log_r, r_h, bh_mass,
+                                                             spin, part);
+  else
+    k_diag_gw<double><<<DIAG_BLOCKS, DIAG_BS, 0, h->stream>>>(h->G, (const double *)h->G.P, dtab, use_log_r, r_h,
+                                                              bh_mass, spin, part);
+  k_sum3_final<<<1, DIAG_BS, 0, h->stream>>>(part, DIAG_BLOCKS, res);
+  if (int rc = launch_check(h)) return rc;
+  double I[3];
+  CUDA_TRY(h, cudaMemcpyAsync(I, res, sizeof I, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));  // the host table goes out of scope
+  out[0] = (I[0] - I[1]) / 1000.0;  // gw_observer_distance, output.f90:28
+  out[1] = (2.0 * I[2]) / 1000.0;
+  out[2] = I[0]; out[3] = I[1]; out[4] = I[2];
   return GRHD2_OK;
 }
 

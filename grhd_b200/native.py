@@ -95,6 +95,8 @@ GPU_SYMBOLS = {
     "grhd2_gpu_upload_async": (C.c_int, [_VP, c_double_p, c_double_p]),
     "grhd2_gpu_global_diagnostics": (C.c_int, [_VP, C.POINTER(Diagnostics)]),
     "grhd2_gpu_snapshot_begin": (C.c_int, [_VP, c_double_p]),
+    "grhd2_gpu_gw_strain": (C.c_int, [_VP, c_double_p, c_double_p, c_double_p, C.c_int, C.c_double, C.c_double,
+                                      c_double_p]),
     "grhd2_gpu_vtk_cell_data": (C.c_int, [_VP, c_double_p, _VP]),
     "grhd2_gpu_snapshot_wait": (C.c_int, [_VP]),
     "grhd2_gpu_total_mass": (C.c_int, [_VP, c_double_p]),

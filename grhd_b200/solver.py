@@ -157,6 +157,16 @@ class GpuGrid:
         self._check(self.lib.grhd2_gpu_ppi_modes(self._h, N.dptr(z), N.dptr(out)))
         return out
 
+    def gw_strain(self) -> np.ndarray:
+        """calc_gw_strain (output.f90:852): h_plus, h_cross, Ixx, Iyy, Ixy of the resident state."""
+        pb = self.problem
+        x, y, z = (np.ascontiguousarray(a[pb.ng + 1:pb.ng + 1 + n]) for a, n in zip(pb.coords(), (pb.nx, pb.ny, pb.nz)))
+        spin = pb.info.a_spin if self.cfg.metric_kind == 2 else 0.0
+        out = np.zeros(5)
+        self._check(self.lib.grhd2_gpu_gw_strain(self._h, N.dptr(x), N.dptr(y), N.dptr(z), int(self.cfg.use_log_r),
+                                                 pb.info.bh_mass, spin, N.dptr(out)))
+        return out
+
     def vtk_cell_data(self) -> np.ndarray:
         """The 7 big-endian cell fields of a VTK frame (output.f90:398-453), shape
         (7, nz, ny, nx), dtype '>f8'; v^r and beta^r scaled by exp(x) on log-r grids."""

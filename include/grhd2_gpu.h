@@ -169,6 +169,12 @@ int grhd2_gpu_vtk_cell_data(grhd2_gpu *h, const double *r_scale, void *out_host)
  * the copy).  A new begin waits on the device for the previous copy. */
 int grhd2_gpu_snapshot_begin(grhd2_gpu *h, double *up_host);
 int grhd2_gpu_snapshot_wait(grhd2_gpu *h);
+/* calc_gw_strain (output.f90:852-948) without its file output: out = h_plus, h_cross and
+ * the quadrupole sums Ixx_ddot, Iyy_ddot, Ixy_ddot.  x, y, z: cell-centre coordinates
+ * (1:nx), (1:ny), (1:nz); spin: the Kerr-Schild spin (0 for Eddington-Finkelstein).  All
+ * zero when the metric is Minkowski or bh_mass < 0.1 (the reference writes nothing then). */
+int grhd2_gpu_gw_strain(grhd2_gpu *h, const double *x, const double *y, const double *z, int use_log_r,
+                        double bh_mass, double spin, double *out);
 /* Asynchronous upload / download (no reference counterpart): the same copies and layout
  * conversions, enqueued on the handle's stream without waiting.  The host arrays must stay
  * valid and unchanged until the stream has finished (grhd2_gpu_synchronize); page-locked

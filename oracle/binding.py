@@ -74,6 +74,7 @@ def lib(libm_exp: bool = False):
             "orc_num_threads": (C.c_int, []),
             "orc_exp": (C.c_double, [C.c_double]),
             "orc_total_mass": (C.c_double, [P, _dp]),
+            "orc_gw_strain": (C.c_int, [P, M, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double, _dp]),
             "orc_mdot": (C.c_int, [P, M, _dp, _dp, C.c_int, _dp]),
             "orc_ppi_modes": (None, [P, _dp, _dp, _dp, _dp]),
             "orc_global_diagnostics": (None, [P, M, _dp, _dp, _dp, C.POINTER(C.c_int64)]),
@@ -181,6 +182,16 @@ class OracleRun:
     def ppi_modes(self, z: np.ndarray) -> np.ndarray:
         out = np.zeros(17)
         self.L.orc_ppi_modes(C.byref(self.cfg), _p(self.up), _p(self.p), _p(np.ascontiguousarray(z)), _p(out))
+        return out
+
+    def gw_strain(self, use_log_r: bool, bh_mass: float, spin: float) -> np.ndarray:
+        pb = self.problem
+        x, y, z = (np.ascontiguousarray(a[pb.ng + 1:pb.ng + 1 + n]) for a, n in zip(pb.coords(), (pb.nx, pb.ny, pb.nz)))
+        out = np.zeros(5)
+        rc = self.L.orc_gw_strain(C.byref(self.cfg), C.byref(self.met), _p(self.p), _p(x), _p(y), _p(z),
+                                  int(use_log_r), bh_mass, spin, _p(out))
+        if rc < 0:
+            raise ValueError("undefined horizon radius")
         return out
 
     def global_diagnostics(self) -> dict:

@@ -1526,3 +1526,67 @@ void orc_global_diagnostics(const orc_config *c, const orc_metric *m, const doub
   f[3] = rmin; f[4] = pmin; f[5] = rmax_; f[6] = pmax; f[7] = vmax;
   n[0] = atmosphere; n[1] = invalid;
 }
+
+/* metrics.f90:66-87 */
+static int horizon_radius(double mass, double spin, double *r_plus) {
+  if (mass < 0.0) return -1;
+  double big = 1.0;
+  if (mass * mass > big) big = mass * mass;
+  if (spin * spin > big) big = spin * spin;
+  const double tol = 64.0 * DBL_EPSILON * big;
+  const double disc = mass * mass - spin * spin;
+  if (disc < -tol) return -1;
+  *r_plus = mass + sqrt(disc > 0.0 ? disc : 0.0);
+  return 0;
+}
+
+/* output.f90:743-768, 797-834, 837-850, 852-948 */
+int orc_gw_strain(const orc_config *c, const orc_metric *m, const double *p, const double *xc, const double *yc,
+                  const double *zc, int use_log_r, double bh_mass, double spin, double *out) {
+  for (int q = 0; q < 5; ++q) out[q] = 0.0;
+  if (c->metric_kind == ORC_METRIC_MINKOWSKI || bh_mass < 0.1) return 1;
+  double r_h;
+  if (horizon_radius(bh_mass, spin, &r_h)) return -1;
+  const lay_t L = mklay(c);
+  double ixx = 0.0, iyy = 0.0, ixy = 0.0;
+  for (int k = 1; k <= c->nz; ++k)
+    for (int j = 1; j <= c->ny; ++j)
+      for (int i = 1; i <= c->nx; ++i) {
+        const double r = use_log_r ? exp(xc[i - 1]) : xc[i - 1];
+        if (r <= r_h) continue;
+        const double th = yc[j - 1], ph = zc[k - 1];
+        double rho = p[pidx(&L, 0, i, j, k)], pres = p[pidx(&L, 1, i, j, k)];
+        rho = rho - c->rho_floor; if (!(rho > 0.0)) rho = 0.0;  /* max(0, rho - rho_floor) */
+        pres = pres - c->p_floor; if (!(pres > 0.0)) pres = 0.0;
+        if (rho <= 0.0 && pres <= 0.0) continue;
+        const size_t q = cell(c, i, j);
+        const double alpha = m->alpha_c[q];
+        double rates[3];
+        for (int d = 0; d < 3; ++d) rates[d] = alpha * p[pidx(&L, 2 + d, i, j, k)] - m->beta_c[3 * q + d];
+        if (use_log_r) rates[0] = r * rates[0];
+        const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+        double pos[3], vel[3];
+        if (fabs(st) <= 64.0 * DBL_EPSILON) {
+          pos[0] = 0.0; pos[1] = 0.0; pos[2] = copysign(fabs(r), ct);
+        } else {
+          pos[0] = (r * cp - spin * sp) * st;
+          pos[1] = (r * sp + spin * cp) * st;
+          pos[2] = r * ct;
+        }
+        vel[0] = rates[0] * cp * st + rates[1] * (r * cp - spin * sp) * ct - rates[2] * (r * sp + spin * cp) * st;
+        vel[1] = rates[0] * sp * st + rates[1] * (r * sp + spin * cp) * ct + rates[2] * (r * cp - spin * sp) * st;
+        vel[2] = rates[0] * ct - r * rates[1] * st;
+        const double sigma = r * r + spin * spin * (ct * ct);
+        const double jac = sigma * st;
+        const double dV = jac * (use_log_r ? r : 1.0) * c->dx * c->dy * c->dz;
+        const double r2 = pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2];
+        const double mr3 = bh_mass / (r2 * sqrt(r2));
+        ixx = ixx + (2.0 * rho * (vel[0] * vel[0]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[0] * pos[0])) * dV;
+        iyy = iyy + (2.0 * rho * (vel[1] * vel[1]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[1] * pos[1])) * dV;
+        ixy = ixy + (2.0 * rho * vel[0] * vel[1] - 2.0 * rho * mr3 * pos[0] * pos[1]) * dV;
+      }
+  out[0] = (ixx - iyy) / 1000.0;
+  out[1] = (2.0 * ixy) / 1000.0;
+  out[2] = ixx; out[3] = iyy; out[4] = ixy;
+  return 0;
+}

@@ -119,6 +119,13 @@ void orc_ppi_modes(const orc_config *c, const double *up, const double *p, const
  * n = atmosphere_cells, invalid_cells */
 void orc_global_diagnostics(const orc_config *c, const orc_metric *m, const double *up, const double *p,
                             double *f, int64_t *n);
+/* output.f90:852-948 calc_gw_strain (Finn-Evans quadrupole proxy, observer at 1000 M,
+ * cells inside the horizon and the numerical atmosphere excluded): out = h_plus, h_cross,
+ * Ixx_ddot, Iyy_ddot, Ixy_ddot; xc, yc, zc the cell centres (1:n); spin the KS spin (0 for
+ * EF).  Returns 0, 1 when the reference skips (Minkowski or bh_mass < 0.1), or -1 when
+ * the horizon radius is undefined (metrics.f90:66-87). */
+int orc_gw_strain(const orc_config *c, const orc_metric *m, const double *p, const double *xc, const double *yc,
+                  const double *zc, int use_log_r, double bh_mass, double spin, double *out);
 /* number of OpenMP threads used by orc_run / orc_step (1 without OpenMP) */
 int orc_num_threads(void);
 /* the exp used by WENO3 (reconstruction.f90:169), exposed for its accuracy test */

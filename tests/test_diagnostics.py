@@ -102,3 +102,75 @@ def test_gpu_diagnostics_match_oracle(maker, kw, steps, precision):
         with pytest.raises(GpuError):
             g.mdot(pb.nx + 1)
     g.close()
+
+
+def numpy_gw(pb, o, spin):
+    """calc_gw_strain (output.f90:852-948) vectorised: Ixx, Iyy, Ixy."""
+    cfg = o.cfg
+    g = pb.ng
+    x, y, z = (a[g + 1:g + 1 + n] for a, n in zip(pb.coords(), (pb.nx, pb.ny, pb.nz)))
+    log_r = bool(pb.config(0).use_log_r)
+    r = (np.exp(x) if log_r else x)[None, None, :]
+    m_bh = pb.info.bh_mass
+    r_h = m_bh + np.sqrt(max(0.0, m_bh * m_bh - spin * spin))
+    q = interior(pb, o.p)
+    rho = np.maximum(q[..., 0] - cfg.rho_floor, 0.0)
+    pres = np.maximum(q[..., 1] - cfg.p_floor, 0.0)
+    mv = pb.metric_view()
+    alpha = np.ctypeslib.as_array(mv.alpha_c, shape=(pb.ny, pb.nx))[None]
+    beta = np.ctypeslib.as_array(mv.beta_c, shape=(pb.ny, pb.nx, 3))[None]
+    rates = alpha[..., None] * q[..., 2:5] - beta
+    if log_r:
+        rates[..., 0] = r * rates[..., 0]
+    st, ct = np.sin(y)[None, :, None], np.cos(y)[None, :, None]
+    sp, cp = np.sin(z)[:, None, None], np.cos(z)[:, None, None]
+    pole = np.abs(st) <= 64 * np.finfo(float).eps
+    pos0 = np.where(pole, 0.0, (r * cp - spin * sp) * st)
+    pos1 = np.where(pole, 0.0, (r * sp + spin * cp) * st)
+    pos2 = np.where(pole, np.copysign(np.abs(r), ct), r * ct)
+    v0 = rates[..., 0] * cp * st + rates[..., 1] * (r * cp - spin * sp) * ct - rates[..., 2] * (r * sp + spin * cp) * st
+    v1 = rates[..., 0] * sp * st + rates[..., 1] * (r * sp + spin * cp) * ct + rates[..., 2] * (r * cp - spin * sp) * st
+    dV = (r * r + spin * spin * ct * ct) * st * (r if log_r else 1.0) * cfg.dx * cfg.dy * cfg.dz
+    r2 = pos0 ** 2 + pos1 ** 2 + pos2 ** 2
+    mr3 = m_bh / (r2 * np.sqrt(r2))
+    keep = (r > r_h) & ~((rho <= 0) & (pres <= 0))
+    ixx = ((2 * rho * v0 ** 2 + 2 * pres - 2 * rho * mr3 * pos0 ** 2) * dV)[keep].sum()
+    iyy = ((2 * rho * v1 ** 2 + 2 * pres - 2 * rho * mr3 * pos1 ** 2) * dV)[keep].sum()
+    ixy = ((2 * rho * v0 * v1 - 2 * rho * mr3 * pos0 * pos1) * dV)[keep].sum()
+    return np.array([ixx, iyy, ixy])
+
+
+GW_CASES = [(torus_3d, dict(nx=24, ny=12, nz=12), 3), (torus_2p5d, dict(nx=64, nz=32), 5), (michel, dict(nx=128), 20)]
+
+
+def _spin(pb):
+    return pb.info.a_spin if pb.config(0).metric_kind == 2 else 0.0
+
+
+@pytest.mark.parametrize("maker,kw,steps", GW_CASES)
+def test_oracle_gw_matches_numpy(maker, kw, steps):
+    pb, o, _ = oracle_state(maker, kw, steps)
+    spin = _spin(pb)
+    got = o.gw_strain(bool(pb.config(0).use_log_r), pb.info.bh_mass, spin)
+    want = numpy_gw(pb, o, spin)
+    scale = np.abs(want).max()
+    assert scale > 0 and np.allclose(got[2:], want, rtol=0, atol=1e-10 * scale)
+    assert got[0] == (got[2] - got[3]) / 1000.0 and got[1] == 2.0 * got[4] / 1000.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("maker,kw,steps", GW_CASES)
+def test_gpu_gw_matches_oracle(maker, kw, steps, precision):
+    from grhd_b200.solver import GpuGrid
+    pb, o, _ = oracle_state(maker, kw, steps)
+    g = GpuGrid(pb, precision=precision, upload_initial=False)
+    g.upload(p=initial_state(pb))
+    g.prim_to_cons()
+    g.run(0.0, 1e30, steps)
+    got = g.gw_strain()
+    want = o.gw_strain(bool(pb.config(0).use_log_r), pb.info.bh_mass, _spin(pb))
+    scale = np.abs(want[2:]).max()
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.allclose(got[2:], want[2:], rtol=0, atol=tol * scale), (got, want)
+    g.close()
