@@ -1602,6 +1602,15 @@ int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *variants, int *t
   cudaEvent_t e0, e1;
   BCUDA_TRY(b, cudaEventCreate(&e0));
   BCUDA_TRY(b, cudaEventCreate(&e1));
+  // In a step the face kernels find little of their input in L2 (the other kernels of the
+  // step evict it); timing repeated launches would favour whichever variant reuses the most.
+  // Each timed repetition therefore starts after a write larger than L2.
+  const size_t flush_bytes = (size_t)160 << 20;
+  void *flush = nullptr;
+  if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    flush = nullptr;  // tune without flushing
+  }
   int rc = 0, k = 0;
   const int ngroups = (int)b->groups.size();
   for (int gi = 0; gi < ngroups && !rc; ++gi) {
@@ -1619,14 +1628,19 @@ int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *variants, int *t
             return grp.mixed ? enqueue_dir<float, float>(b, grp, d, v) : enqueue_dir<double, double>(b, grp, d, v);
           };
           if ((rc = run())) break;  // warm-up
-          cudaEventRecord(e0, b->stream);
-          for (int r = 0; r < reps && !rc; ++r) rc = run();
-          cudaEventRecord(e1, b->stream);
-          if (rc) break;
-          cudaError_t e = cudaEventSynchronize(e1);
-          if (e != cudaSuccess) { rc = bfail(b, GRHD2_ERR_CUDA, "autotune: %s", cudaGetErrorString(e)); break; }
           float t = 0.0f;
-          cudaEventElapsedTime(&t, e0, e1);
+          for (int r = 0; r < reps && !rc; ++r) {
+            if (flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes, b->stream);
+            cudaEventRecord(e0, b->stream);
+            rc = run();
+            cudaEventRecord(e1, b->stream);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) { rc = bfail(b, GRHD2_ERR_CUDA, "autotune: %s", cudaGetErrorString(e)); break; }
+            float tr = 0.0f;
+            cudaEventElapsedTime(&tr, e0, e1);
+            t += tr;
+          }
+          if (rc) break;
           if (first || t < best) { best = t; best_c = FluxChoice{v, tx}; first = false; }
         }
         if (rc) break;
@@ -1646,6 +1660,10 @@ int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *variants, int *t
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (flush) {
+    cudaStreamSynchronize(b->stream);
+    cudaFree(flush);
+  }
   b->forced.clear();  // the choices now come from the cache
   int rc2 = build_batch(b);
   for (int g = 0; g < n; ++g)
