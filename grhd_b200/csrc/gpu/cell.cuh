@@ -31,9 +31,9 @@ __device__ __forceinline__ void sources(const GridDev &G, const Phys &P, long lo
   const R W = R(1) / sqrt(R(1) - vsq);
   R uf[4];
   uf[0] = W / alpha;
-  uf[1] = W * (v[0] - ld(CF_B1) / alpha);
-  uf[2] = W * (v[1] - ld(CF_B2) / alpha);
-  uf[3] = W * (v[2] - ld(CF_B3) / alpha);
+  uf[1] = W * (v[0] - ld(CF_VA));  // beta^i / alpha: per (i,j), rounded once (the same quotient)
+  uf[2] = W * (v[1] - ld(CF_VA + 1));
+  uf[3] = W * (v[2] - ld(CF_VA + 2));
   R T[10];
 #pragma unroll
   for (int mu = 0; mu <= 3; ++mu)

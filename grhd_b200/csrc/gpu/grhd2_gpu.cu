@@ -823,7 +823,7 @@ int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m) {
         }
       }
     for (int mu = 0; mu < 4; ++mu) C[(CF_DLNA + mu) * nij + q] = m->dlna_c[4 * q + mu];
-    C[CF_VA * nij + q] = m->beta_c[3 * q] / m->alpha_c[q];
+    for (int d = 0; d < 3; ++d) C[(CF_VA + d) * nij + q] = m->beta_c[3 * q + d] / m->alpha_c[q];
   }
   const double eps64 = 64.0 * DBL_EPSILON;
   std::vector<double> T[3];

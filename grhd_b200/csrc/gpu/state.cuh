@@ -29,8 +29,10 @@ enum CentreField {
   CF_CH0 = 27,   // Gamma^0_{mu nu}, 10 symmetric entries
   CF_DG = 37,    // d_d g_{mu nu}, d = 1..3, 10 symmetric entries each
   CF_DLNA = 67,  // d_mu ln(alpha), 4 entries
-  CF_VA = 71,    // beta^1 / alpha (shift-aware outflow clamp, conditions.f90:926)
-  NCF = 72
+  CF_VA = 71,    // beta^i / alpha, i = 1..3 (the shift-aware outflow clamp, conditions.f90:926,
+                 // and the four-velocity of the sources, metrics.f90:1251-1310): the quotient
+                 // of the same operands the reference divides per cell, rounded once
+  NCF = 74
 };
 // face table fields (per face of one direction)
 enum FaceField {
