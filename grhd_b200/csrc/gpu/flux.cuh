@@ -141,9 +141,9 @@ __device__ __forceinline__ void recon_one(int br, int lim, const R (&s)[6], R &q
 // Resident blocks per SM the register allocation must allow (256-thread recon blocks,
 // 128-thread Riemann blocks).  Both kernels stall on dependent FP64 chains, so occupancy
 // pays more than the few registers it costs: measured on the batched 2.5D torus and the
-// 3D torus, 4 recon blocks (64 registers) and 8 Riemann blocks (64 registers) are fastest.
+// 3D torus, 5 recon blocks (51 registers) and 8 Riemann blocks (64 registers) are fastest.
 #ifndef GRHD_RECON_MIN_BLOCKS
-#define GRHD_RECON_MIN_BLOCKS 4
+#define GRHD_RECON_MIN_BLOCKS 5
 #endif
 #ifndef GRHD_RIEMANN_MIN_BLOCKS
 #define GRHD_RIEMANN_MIN_BLOCKS 8
