@@ -385,10 +385,13 @@ def run_serve(args):
     from grhd_b200.serve import GpuEngine, SolveServer, make_stream, summarize
     reqs = make_stream(args.serve_requests, seed=20260901, rate=args.serve_rate,
                        michel_final_time=args.serve_michel_final_time)
-    srv = SolveServer(GpuEngine("fp64"), steps_per_round=16)
+    eng = GpuEngine("fp64")
+    srv = SolveServer(eng, steps_per_round=16)
     res = srv.run(reqs)
+    eng.close()
     out = summarize(res)
     out.update(peak_active=srv.peak_active, rounds=srv.rounds, batch_rebuilds=srv.rebuilds,
+               host_s={k: round(v, 3) for k, v in {**srv.host_s, **eng.host_s}.items()},
                sample=f"{args.serve_requests} requests of the 4096-request stream (seed 20260901), "
                       f"{args.serve_rate:g} arrivals/s, Michel final time {args.serve_michel_final_time:g} M, FP64",
                timing="wall clock from each arrival to its result on the host")

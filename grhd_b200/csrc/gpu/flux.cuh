@@ -71,6 +71,18 @@ __device__ __forceinline__ double load_var(const PT *__restrict__ P, const GridD
   return out;
 }
 
+// Stencil window m = lo..hi (cells face-2+m along DIR; 0 elsewhere) of variable v for a
+// face whose window leaves the grid: boundary fill on load.  The fused face kernel calls
+// it out of line, so its interior path keeps the registers for the reconstruction and
+// the Riemann solver (measured: mixed 2.5D torus batch +7 %, 3D torus +16 %).  k_recon
+// keeps the boundary fill inline: the call costs its FP64 interior path 7 %.
+template <int DIR, class R, class PT>
+__device__ __noinline__ void edge_stencil(const PT *__restrict__ P, const GridDev &G, const FaceIndex &x, int v, int lo,
+                                          int hi, R (&s)[6]) {
+#pragma unroll
+  for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? R(load_var<DIR>(P, G, x, x.face - 2 + m, v)) : R(0);
+}
+
 // branch selection of reconstruct_1d_core from the density and pressure stencils
 // rho[m], p[m] = prim(., i-2+m), m = 0..4
 template <int REC, class R>
@@ -245,17 +257,30 @@ __device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned
     const int c0 = x.face - 2 + lo;
     base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
   }
-  auto ld = [&](int v, int m) -> R {
-    return inside ? R((double)GRHD_LDP(&Pin[v * G.pplane + base + m * stride]))
-                  : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, v));
+  // window m = a..b of variable w; the interior case reads P at a fixed stride
+  auto window = [&](int w, int a, int b, R(&out)[6]) {
+    if (inside) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m)
+        out[m] = (m >= a && m <= b) ? R((double)GRHD_LDP(&Pin[w * G.pplane + base + m * stride])) : R(0);
+    } else {
+      edge_stencil<DIR>(Pin, G, x, w, a, b, out);
+    }
   };
   int br = BR_GODUNOV;
   if (REC != REC_GODUNOV) {
     R rho[5], pr[5];
+    if (P.sensor) {  // the sensor reads cells 0..4 of the window (inside [lo, hi] when it is on)
+      R t[6];
+      window(EQ_DE, 0, 4, t);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      rho[m] = P.sensor ? ld(EQ_DE, m) : R(0);
-      pr[m] = P.sensor ? ld(EQ_PR, m) : R(0);
+      for (int m = 0; m < 5; ++m) rho[m] = t[m];
+      window(EQ_PR, 0, 4, t);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) pr[m] = t[m];
+    } else {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { rho[m] = R(0); pr[m] = R(0); }
     }
     br = branch_of<REC>(P, rho, pr, x.face, n, DIR);
   }
@@ -263,8 +288,7 @@ __device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned
 #pragma unroll 1
   for (int v = 0; v < NEQ; ++v) {
     R s[6];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ld(v, m) : R(0);
+    window(v, lo, hi, s);
     R qL, qR;
     recon_one<REC>(br, P.lim, s, qL, qR);
     if (v == EQ_DE || v == EQ_PR) {  // reconstruction.f90:647-655

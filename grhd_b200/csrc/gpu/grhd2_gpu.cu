@@ -187,6 +187,11 @@ struct grhd2_gpu_batch {
   std::map<std::pair<int, int>, FluxChoice> forced;  // (group, direction) -> choice, while tuning
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // a captured step runs the scheme groups as parallel branches of its graph: group 0 on
+  // the batch stream, group g on lanes[g - 1] (forked from and joined back into it)
+  std::vector<cudaStream_t> lanes;
+  std::vector<cudaEvent_t> lane_done;
+  cudaEvent_t fork = nullptr;
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;
   std::vector<const char *> prof_names;
@@ -223,11 +228,34 @@ int bfail(grhd2_gpu_batch *b, int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return bfail((b), GRHD2_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
+// Handle buffers come from the device's stream-ordered memory pool, allocated and freed
+// in the order of the handle's stream: creating and destroying grids (a solve server does
+// this all the time) neither synchronises the device nor returns memory to the driver.
+// The pool keeps up to POOL_KEEP_BYTES of freed memory for reuse.  Every entry point that
+// allocates synchronises the handle's stream before it returns, so the buffers are ready
+// for any stream afterwards.
+constexpr unsigned long long POOL_KEEP_BYTES = 8ull << 30;
+static void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static std::vector<int> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (std::find(done.begin(), done.end(), device) != done.end()) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = POOL_KEEP_BYTES;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done.push_back(device);
+}
+
 template <class T>
 int dalloc(grhd2_gpu *h, T **p, size_t n) {
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
-  if (e != cudaSuccess) return fail(h, GRHD2_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  cudaError_t e = cudaMallocAsync((void **)p, n * sizeof(T), h->stream);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(h, GRHD2_ERR_NOMEM, "cudaMallocAsync(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  }
   return 0;
 }
 
@@ -249,22 +277,26 @@ int blaunch_check(grhd2_gpu_batch *b, const char *name) {
   return 0;
 }
 
+// Descriptor buffers of a batch live in the stream-ordered pool too, released in the
+// order of the batch's stream: a rebuild (grids joining or leaving) frees the old ones
+// after the steps already enqueued and never synchronises the device.
 void destroy_batch_resources(grhd2_gpu_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+  auto release = [b](void *p) { if (p) cudaFreeAsync(p, b->stream); };
   for (auto &g : b->groups) {
-    if (g.d_map) cudaFree(g.d_map);
-    if (g.d_members) cudaFree(g.d_members);
-    if (g.d_seg) cudaFree(g.d_seg);
+    release(g.d_map);
+    release(g.d_members);
+    release(g.d_seg);
   }
-  if (b->d_bar) cudaFree(b->d_bar);
+  release(b->d_bar);
   b->d_bar = nullptr;
   b->groups.clear();
-  if (b->d_grids) cudaFree(b->d_grids);
+  release(b->d_grids);
   b->d_grids = nullptr;
-  if (b->d_clocks) cudaFree(b->d_clocks);
+  release(b->d_clocks);
   b->d_clocks = nullptr;
 }
 
@@ -342,8 +374,8 @@ int build_batch(grhd2_gpu_batch *b) {
       for (int g : grp.members) set_face_tiles(hg[g], d, ch.tx);
     }
   }
-  BCUDA_TRY(b, cudaMalloc((void **)&b->d_grids, sizeof(GridDev) * n));
-  BCUDA_TRY(b, cudaMalloc((void **)&b->d_clocks, sizeof(GridClock) * n));
+  BCUDA_TRY(b, cudaMallocAsync((void **)&b->d_grids, sizeof(GridDev) * n, b->stream));
+  BCUDA_TRY(b, cudaMallocAsync((void **)&b->d_clocks, sizeof(GridClock) * n, b->stream));
   BCUDA_TRY(b, cudaMemcpyAsync(b->d_grids, hg.data(), sizeof(GridDev) * n, cudaMemcpyHostToDevice, b->stream));
   for (auto &grp : b->groups) {
     std::vector<BlockMap> map;
@@ -355,7 +387,7 @@ int build_batch(grhd2_gpu_batch *b) {
       }
       grp.nb[k] = (int)map.size() - grp.off[k];
     }
-    BCUDA_TRY(b, cudaMalloc((void **)&grp.d_map, sizeof(BlockMap) * std::max<size_t>(1, map.size())));
+    BCUDA_TRY(b, cudaMallocAsync((void **)&grp.d_map, sizeof(BlockMap) * std::max<size_t>(1, map.size()), b->stream));
     BCUDA_TRY(b, cudaMemcpyAsync(grp.d_map, map.data(), sizeof(BlockMap) * map.size(), cudaMemcpyHostToDevice, b->stream));
     // persistent kernel: flattened item spaces (faces of every active direction; cells)
     std::vector<Segment> seg;
@@ -375,16 +407,16 @@ int build_batch(grhd2_gpu_batch *b) {
     }
     grp.nseg_cell = (int)seg.size() - grp.nseg_face;
     grp.n_cell = first;
-    BCUDA_TRY(b, cudaMalloc((void **)&grp.d_seg, sizeof(Segment) * seg.size()));
+    BCUDA_TRY(b, cudaMallocAsync((void **)&grp.d_seg, sizeof(Segment) * seg.size(), b->stream));
     BCUDA_TRY(b, cudaMemcpyAsync(grp.d_seg, seg.data(), sizeof(Segment) * seg.size(), cudaMemcpyHostToDevice, b->stream));
-    BCUDA_TRY(b, cudaMalloc((void **)&grp.d_members, sizeof(int) * grp.members.size()));
+    BCUDA_TRY(b, cudaMallocAsync((void **)&grp.d_members, sizeof(int) * grp.members.size(), b->stream));
     BCUDA_TRY(b, cudaMemcpyAsync(grp.d_members, grp.members.data(), sizeof(int) * grp.members.size(),
                                  cudaMemcpyHostToDevice, b->stream));
     cudaError_t e = grp.mixed ? run_persistent<float, float>(grp.rec, grp.rs, true, &grp.max_blocks, {}, 0, 0, b->stream)
                               : run_persistent<double, double>(grp.rec, grp.rs, true, &grp.max_blocks, {}, 0, 0, b->stream);
     if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "persistent kernel occupancy: %s", cudaGetErrorString(e));
   }
-  BCUDA_TRY(b, cudaMalloc((void **)&b->d_bar, 4 * sizeof(unsigned)));
+  BCUDA_TRY(b, cudaMallocAsync((void **)&b->d_bar, 4 * sizeof(unsigned), b->stream));
   BCUDA_TRY(b, cudaMemsetAsync(b->d_bar, 0, 4 * sizeof(unsigned), b->stream));
   // step mode
   b->persistent = b->step_request == GRHD2_STEP_PERSISTENT;
@@ -403,56 +435,98 @@ int refresh_batch(grhd2_gpu_batch *b) {
 
 // kind 0..5 for directions, then the cell kernel in MODE (0 rhs, 1..3 stages)
 template <class R, class PT>
-int enqueue_dir(grhd2_gpu_batch *b, const Group &grp, int d, int variant) {
+int enqueue_dir(grhd2_gpu_batch *b, const Group &grp, int d, int variant, cudaStream_t st) {
   const int kr = 2 * (d - 1), ks = kr + 1, kf = K_FLUX_X + d - 1;
   if (variant == GRHD2_FLUX_FUSED) {
     if (grp.nb[kf] > 0) {
-      launch_flux<R, PT>(d, grp.rec, grp.rs, b->d_grids, grp.d_map + grp.off[kf], grp.nb[kf], b->stream);
+      launch_flux<R, PT>(d, grp.rec, grp.rs, b->d_grids, grp.d_map + grp.off[kf], grp.nb[kf], st);
       if (int rc = blaunch_check(b, KIND_NAME[kf])) return rc;
     }
     return 0;
   }
   if (grp.nb[kr] > 0) {
-    launch_recon<R, PT>(d, grp.rec, b->d_grids, grp.d_map + grp.off[kr], grp.nb[kr], b->stream);
+    launch_recon<R, PT>(d, grp.rec, b->d_grids, grp.d_map + grp.off[kr], grp.nb[kr], st);
     if (int rc = blaunch_check(b, KIND_NAME[kr])) return rc;
   }
   if (grp.nb[ks] > 0) {
-    launch_riemann<R>(d, grp.rs, b->d_grids, grp.d_map + grp.off[ks], grp.nb[ks], b->stream);
+    launch_riemann<R>(d, grp.rs, b->d_grids, grp.d_map + grp.off[ks], grp.nb[ks], st);
     if (int rc = blaunch_check(b, KIND_NAME[ks])) return rc;
   }
   return 0;
 }
 
 template <class R, class PT>
-int enqueue_fluxes(grhd2_gpu_batch *b, const Group &grp) {
+int enqueue_fluxes(grhd2_gpu_batch *b, const Group &grp, cudaStream_t st) {
   for (int d = 1; d <= 3; ++d)
-    if (int rc = enqueue_dir<R, PT>(b, grp, d, grp.variant[d - 1])) return rc;
+    if (int rc = enqueue_dir<R, PT>(b, grp, d, grp.variant[d - 1], st)) return rc;
   return 0;
 }
 
 template <int MODE, class R, class PT>
-int enqueue_cells(grhd2_gpu_batch *b, const Group &grp) {
+int enqueue_cells(grhd2_gpu_batch *b, const Group &grp, cudaStream_t st) {
   if (grp.nb[K_CELL] <= 0) return 0;
-  launch_cell<R, PT>(MODE, b->d_grids, grp.d_map + grp.off[K_CELL], grp.nb[K_CELL], b->stream);
+  launch_cell<R, PT>(MODE, b->d_grids, grp.d_map + grp.off[K_CELL], grp.nb[K_CELL], st);
   return blaunch_check(b, MODE == 0 ? "cell_rhs" : "cell_update");
 }
 
-template <int MODE>
-int enqueue_stage(grhd2_gpu_batch *b) {
-  for (const auto &grp : b->groups) {
-    int rc = grp.mixed ? enqueue_fluxes<float, float>(b, grp) : enqueue_fluxes<double, double>(b, grp);
-    if (rc) return rc;
-    rc = grp.mixed ? enqueue_cells<MODE, float, float>(b, grp) : enqueue_cells<MODE, double, double>(b, grp);
-    if (rc) return rc;
+// the three SSP-RK3 stages of one scheme group (its grids depend on no other group's)
+int enqueue_group_step(grhd2_gpu_batch *b, const Group &grp, cudaStream_t st) {
+  int rc;
+  if (grp.mixed) {
+    if ((rc = enqueue_fluxes<float, float>(b, grp, st)) || (rc = enqueue_cells<1, float, float>(b, grp, st)) ||
+        (rc = enqueue_fluxes<float, float>(b, grp, st)) || (rc = enqueue_cells<2, float, float>(b, grp, st)) ||
+        (rc = enqueue_fluxes<float, float>(b, grp, st)) || (rc = enqueue_cells<3, float, float>(b, grp, st)))
+      return rc;
+  } else {
+    if ((rc = enqueue_fluxes<double, double>(b, grp, st)) || (rc = enqueue_cells<1, double, double>(b, grp, st)) ||
+        (rc = enqueue_fluxes<double, double>(b, grp, st)) || (rc = enqueue_cells<2, double, double>(b, grp, st)) ||
+        (rc = enqueue_fluxes<double, double>(b, grp, st)) || (rc = enqueue_cells<3, double, double>(b, grp, st)))
+      return rc;
   }
   return 0;
 }
 
-int enqueue_step(grhd2_gpu_batch *b) {
-  int rc;
-  if ((rc = enqueue_stage<1>(b))) return rc;
-  if ((rc = enqueue_stage<2>(b))) return rc;
-  if ((rc = enqueue_stage<3>(b))) return rc;
+// streams and events for the branches of a captured step (created before the capture)
+int ensure_lanes(grhd2_gpu_batch *b) {
+  const size_t need = b->groups.empty() ? 0 : b->groups.size() - 1;
+  if (need > 0 && !b->fork) BCUDA_TRY(b, cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  while (b->lanes.size() < need) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    BCUDA_TRY(b, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    b->lanes.push_back(s);
+    BCUDA_TRY(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->lane_done.push_back(e);
+  }
+  return 0;
+}
+
+void destroy_lanes(grhd2_gpu_batch *b) {
+  for (cudaStream_t s : b->lanes) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->lane_done) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  b->lanes.clear();
+  b->lane_done.clear();
+  b->fork = nullptr;
+}
+
+// One step of every grid.  branches: the scheme groups fork off the batch stream and join
+// before the clocks advance (used while capturing the step's graph, where the groups
+// become parallel branches); otherwise they run one after another on the batch stream.
+int enqueue_step(grhd2_gpu_batch *b, bool branches = false) {
+  const int ng = (int)b->groups.size();
+  branches = branches && ng > 1 && (int)b->lanes.size() >= ng - 1;
+  if (branches) {
+    BCUDA_TRY(b, cudaEventRecord(b->fork, b->stream));
+    for (int g = 1; g < ng; ++g) BCUDA_TRY(b, cudaStreamWaitEvent(b->lanes[g - 1], b->fork, 0));
+  }
+  for (int g = 0; g < ng; ++g)
+    if (int rc = enqueue_group_step(b, b->groups[g], branches && g > 0 ? b->lanes[g - 1] : b->stream)) return rc;
+  if (branches)
+    for (int g = 1; g < ng; ++g) {
+      BCUDA_TRY(b, cudaEventRecord(b->lane_done[g - 1], b->lanes[g - 1]));
+      BCUDA_TRY(b, cudaStreamWaitEvent(b->stream, b->lane_done[g - 1], 0));
+    }
   const int n = (int)b->m.size();
   k_advance_clocks<<<nblocks(n, 128), 128, 0, b->stream>>>(b->d_grids, n);
   return blaunch_check(b, "advance_clocks");
@@ -503,8 +577,9 @@ int batch_steps(grhd2_gpu_batch *b, long long nsteps, bool use_graph) {
     return 0;
   }
   if (!b->exec) {
+    if (int rc = ensure_lanes(b)) return rc;
     BCUDA_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_step(b);
+    int rc = enqueue_step(b, true);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -670,6 +745,12 @@ int grhd2_gpu_set_stream(grhd2_gpu *h, void *stream) {
   if (!h) return GRHD2_ERR_ARG;
   CUDA_TRY(h, cudaSetDevice(h->device));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (h->self) {  // the batch of one follows the handle; its graph was captured for the old stream
+    destroy_batch_resources(h->self);  // released in the old stream's order: before it goes
+    destroy_lanes(h->self);
+    delete h->self;
+    h->self = nullptr;
+  }
   if (h->own_stream) CUDA_TRY(h, cudaStreamDestroy(h->stream));
   h->own_stream = false;
   h->stream = nullptr;
@@ -678,11 +759,6 @@ int grhd2_gpu_set_stream(grhd2_gpu *h, void *stream) {
   } else {
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
-  }
-  if (h->self) {  // the batch of one follows the handle; its graph was captured for the old stream
-    destroy_batch_resources(h->self);
-    delete h->self;
-    h->self = nullptr;
   }
   return GRHD2_OK;
 }
@@ -739,6 +815,7 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   G.dx = c.dx; G.dy = c.dy; G.dz = c.dz;
 
   CUDA_TRY(h, cudaGetDevice(&h->device));
+  keep_pool_memory(h->device);
   if (stream) {
     h->stream = (cudaStream_t)stream;
   } else {
@@ -888,7 +965,8 @@ int grhd2_gpu_set_bc_data(grhd2_gpu *h, const grhd2_gpu_bc_view *b) {
     for (size_t q = 0; q < n / 5; ++q)
       for (int v = 0; v < 5; ++v) t[v * (n / 5) + q] = b->michel_injector[5 * q + v];
     if (!h->inj && (rc = dalloc(h, &h->inj, n))) return rc;
-    CUDA_TRY(h, cudaMemcpy(h->inj, t.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpyAsync(h->inj, t.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));  // in the handle's stream order; the source is released
     h->G.inj = h->inj;
   }
   if (c.case_id == 8) {
@@ -898,14 +976,16 @@ int grhd2_gpu_set_bc_data(grhd2_gpu *h, const grhd2_gpu_bc_view *b) {
     for (int g = 0; g < c.nghost; ++g)
       for (int v = 0; v < 5; ++v) t[v * c.nghost + g] = b->dust_outer[5 * g + v];
     if (!h->dust && (rc = dalloc(h, &h->dust, n))) return rc;
-    CUDA_TRY(h, cudaMemcpy(h->dust, t.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpyAsync(h->dust, t.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));  // in the handle's stream order; the source is released
     h->G.dust = h->dust;
   }
   if (c.case_id == 5) {
     if (!b->x_c) return fail(h, GRHD2_ERR_ARG, "jet case needs x_c");
     const size_t n = (size_t)c.nx + 2 * c.nghost + 1;
     if (!h->xc && (rc = dalloc(h, &h->xc, n))) return rc;
-    CUDA_TRY(h, cudaMemcpy(h->xc, b->x_c, n * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpyAsync(h->xc, b->x_c, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));  // in the handle's stream order; the source is released
     h->G.xc = h->xc;
   }
   for (int q = 0; q < 7; ++q) h->G.jet[q] = b->jet[q];
@@ -1033,8 +1113,9 @@ int grhd2_gpu_calc_rhs(grhd2_gpu *h, double *rhs_host) {
   if ((rc = write_clock(h))) return rc;
   grhd2_gpu_batch *b = h->self;
   for (const auto &grp : b->groups) {
-    rc = grp.mixed ? enqueue_fluxes<float, float>(b, grp) : enqueue_fluxes<double, double>(b, grp);
-    if (!rc) rc = grp.mixed ? enqueue_cells<0, float, float>(b, grp) : enqueue_cells<0, double, double>(b, grp);
+    rc = grp.mixed ? enqueue_fluxes<float, float>(b, grp, b->stream) : enqueue_fluxes<double, double>(b, grp, b->stream);
+    if (!rc)
+      rc = grp.mixed ? enqueue_cells<0, float, float>(b, grp, b->stream) : enqueue_cells<0, double, double>(b, grp, b->stream);
     if (rc) return fail(h, rc, "%s", b->err.c_str());
   }
   if (rhs_host) {
@@ -1123,9 +1204,13 @@ static int faces_common(grhd2_gpu *h, int n, int dir, const double *qL, const do
   std::vector<double> T;
   if (int rc = build_face_table(h, T, (size_t)n, dir, alpha, beta, gamma, sqg, {})) return rc;
   double *dT = nullptr, *dq = nullptr;
-  int rc;
-  if ((rc = dalloc(h, &dT, T.size()))) return rc;
-  if ((rc = dalloc(h, &dq, (size_t)15 * n))) { cudaFree(dT); return rc; }
+  // scratch of this call only, on the legacy stream like the copies below
+  if (cudaMalloc((void **)&dT, T.size() * sizeof(double)) != cudaSuccess)
+    return fail(h, GRHD2_ERR_NOMEM, "cudaMalloc of the face table failed");
+  if (cudaMalloc((void **)&dq, (size_t)15 * n * sizeof(double)) != cudaSuccess) {
+    cudaFree(dT);
+    return fail(h, GRHD2_ERR_NOMEM, "cudaMalloc of the face states failed");
+  }
   cudaMemcpy(dT, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice);
   cudaMemcpy(dq, qL, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice);
   if (qR) cudaMemcpy(dq + 5 * n, qR, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice);
@@ -1460,6 +1545,7 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->self) {
     destroy_batch_resources(h->self);
+    destroy_lanes(h->self);
     delete h->self;
   }
   if (h->snap_stream) {
@@ -1468,13 +1554,12 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
   }
   if (h->snap_taken) cudaEventDestroy(h->snap_taken);
   if (h->snap_done) cudaEventDestroy(h->snap_done);
-  if (h->snap) cudaFree(h->snap);
-  if (h->vtk) cudaFree(h->vtk);
   void *bufs[] = {h->G.P, h->G.U, h->G.UP, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1], h->G.F[2], h->G.cnt, h->G.clock,
                   h->centre, h->face[0], h->face[1], h->face[2], h->centre_f, h->face_f[0], h->face_f[1], h->face_f[2],
                   h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],
-                  h->frozen[2], h->red, h->staging, h->diag};
-  for (void *b : bufs) if (b) cudaFree(b);
+                  h->frozen[2], h->red, h->staging, h->diag, h->snap, h->vtk};
+  // stream-ordered release: after the handle's stream (synchronised above) has drained
+  for (void *b : bufs) if (b) cudaFreeAsync(b, h->stream);
   if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1625,7 +1710,8 @@ int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *variants, int *t
           if ((rc = build_batch(b))) break;
           const Group &grp = b->groups[gi];
           auto run = [&]() {
-            return grp.mixed ? enqueue_dir<float, float>(b, grp, d, v) : enqueue_dir<double, double>(b, grp, d, v);
+            return grp.mixed ? enqueue_dir<float, float>(b, grp, d, v, b->stream)
+                             : enqueue_dir<double, double>(b, grp, d, v, b->stream);
           };
           if ((rc = run())) break;  // warm-up
           float t = 0.0f;
@@ -1688,6 +1774,7 @@ void grhd2_gpu_batch_destroy(grhd2_gpu_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   destroy_batch_resources(b);
+  destroy_lanes(b);
   delete b;
 }
 

@@ -94,6 +94,15 @@ class Problem:
         ptr = self._lib.grhd2_problem_prims(self._h)
         return np.ctypeslib.as_array(ptr, shape=(n,)).copy().reshape(self.prim_shape)
 
+    def prims_view(self) -> np.ndarray:
+        """The initial ghosted primitives in the problem's own buffer (no copy; valid while
+        the problem lives and only to be read)."""
+        n = self._lib.grhd2_problem_prim_size(self._h)
+        ptr = self._lib.grhd2_problem_prims(self._h)
+        v = np.ctypeslib.as_array(ptr, shape=(n,)).reshape(self.prim_shape)
+        v.flags.writeable = False
+        return v
+
     def perturb(self, p: np.ndarray) -> np.ndarray:
         """Apply the configured perturbation to a ghosted primitive array in place."""
         assert p.shape == self.prim_shape and p.dtype == np.float64

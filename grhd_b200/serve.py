@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import collections
+import concurrent.futures
 import dataclasses
 import json
 import math
@@ -98,25 +99,47 @@ class Result:
 
 # ------------------------------------------------------------------------------------
 class GpuEngine:
-    """Grids and batches on the GPU through the C-ABI (grhd_b200.solver)."""
+    """Grids and batches on the GPU through the C-ABI (grhd_b200.solver).
 
-    def __init__(self, precision: str = "fp64", device: int = 0):
+    The host-side set-up of a request (grid, metric tables, initial data: milliseconds of
+    host work per request) runs on a pool of host threads from the moment the request
+    arrives, so admission only waits for it when it has not finished yet."""
+
+    def __init__(self, precision: str = "fp64", device: int = 0, host_workers: int = 8):
         import torch
         torch.cuda.set_device(device)
         self.torch = torch
         self.precision = precision
         self.stream = torch.cuda.Stream(device=device)
-        self._problems = {}
+        self._problems = {}  # request id -> Future of its Problem
+        self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=host_workers)
+        self.retire_stream = torch.cuda.Stream(device=device)
+        # host seconds: waiting for a set-up, GPU grid creation (buffers, tables), initial
+        # data (upload, prim_to_cons, first CFL), result + release, and the parts of a
+        # batch rebuild
+        self.host_s = dict(setup_wait=0.0, create=0.0, upload=0.0, retire=0.0, batch_close=0.0, batch_join=0.0,
+                           batch_create=0.0, batch_clock=0.0)
+
+    def close(self):
+        self._pool.shutdown(wait=True)
 
     def free_bytes(self) -> int:
         return int(self.torch.cuda.mem_get_info()[0])
 
-    def problem(self, req: Request):
-        """The request's host-side set-up (metric tables, initial data), built once."""
+    def announce(self, req: Request):
+        """Start the request's host-side set-up on the thread pool (ctypes releases the
+        GIL while the host library builds it)."""
         from .problem import Problem
         if req.id not in self._problems:
-            self._problems[req.id] = Problem.from_keys(req.problem, **req.keys)
-        return self._problems[req.id]
+            self._problems[req.id] = self._pool.submit(Problem.from_keys, req.problem, **req.keys)
+
+    def problem(self, req: Request):
+        """The request's host-side set-up (metric tables, initial data), built once."""
+        self.announce(req)
+        ts = time.perf_counter()
+        pb = self._problems[req.id].result()
+        self.host_s["setup_wait"] += time.perf_counter() - ts
+        return pb
 
     def bytes_needed(self, req: Request) -> int:
         from . import native as N
@@ -128,23 +151,34 @@ class GpuEngine:
         from .solver import GpuGrid
         pb = self.problem(req)
         del self._problems[req.id]
+        ts = time.perf_counter()
         g = GpuGrid(pb, precision=self.precision, upload_initial=False)
-        g.upload(p=pb.initial_prims())
+        tu = time.perf_counter()
+        g.upload(p=pb.prims_view())
         g.prim_to_cons()
         g.cfl()
+        te = time.perf_counter()
+        self.host_s["create"] += tu - ts
+        self.host_s["upload"] += te - tu
         return g
 
     def batch(self, grids, new_clocks):
         """Batch of the resident grids on the batch stream; new_clocks[k] = (t0, final) for
         grids that join now (None for grids keeping their running clock)."""
         from .solver import GpuBatch
+        t = [time.perf_counter()]
         for g in grids:
             if g.stream_ptr != self.stream.cuda_stream:
                 g.set_stream(self.stream.cuda_stream)
+        t.append(time.perf_counter())
         b = GpuBatch(grids)
+        t.append(time.perf_counter())
         for k, c in enumerate(new_clocks):
             if c is not None:
                 b.set_clock(k, c[0], c[1], -1)
+        t.append(time.perf_counter())
+        for key, a, z in (("batch_join", 0, 1), ("batch_create", 1, 2), ("batch_clock", 2, 3)):
+            self.host_s[key] += t[z] - t[a]
         return b
 
     def step(self, batch, nsteps: int):
@@ -153,13 +187,22 @@ class GpuEngine:
     def clocks(self, batch):
         return batch.clocks()
 
+    def detach(self, grid):
+        """Move a finished grid off the batch stream (which is idle after the round's clock
+        read), so its result can be read while the next round runs."""
+        grid.set_stream(self.retire_stream.cuda_stream)
+
     def finish(self, grid, keep: bool):
+        ts = time.perf_counter()
         up = grid.download(want_p=False)[0] if keep else None
         grid.close()
+        self.host_s["retire"] += time.perf_counter() - ts
         return up
 
     def close_batch(self, batch):
+        ts = time.perf_counter()
         batch.close()
+        self.host_s["batch_close"] += time.perf_counter() - ts
 
 
 class SolveServer:
@@ -178,6 +221,8 @@ class SolveServer:
         self.peak_active = 0
         self.rounds = 0
         self.rebuilds = 0
+        # host seconds per activity: where a round's wall clock goes
+        self.host_s = dict(prepare=0.0, enqueue=0.0, wait=0.0, retire=0.0, rebuild=0.0)
 
     def run(self, requests: list[Request]) -> list[Result]:
         eng = self.engine
@@ -185,18 +230,34 @@ class SolveServer:
         waiting = collections.deque()
         active = []        # [request, grid, bytes, admitted time]
         new_clock = []     # parallel to active: (t0, final) until the grid joins a batch
+        retiring = []      # finished: [request, grid, bytes, admitted time, steps, t]
         results = []
         used = 0
         batch = None
         changed = False
         t0 = self.clock()
-        while pending or waiting or active:
+        while pending or waiting or active or retiring:
             if batch is not None:
+                ts = self.clock()
                 eng.step(batch, self.k)  # asynchronous: host work below overlaps it
+                self.host_s["enqueue"] += self.clock() - ts
                 self.rounds += 1
+            # results of the grids that finished in the previous round, read while this
+            # round runs; their memory returns to the budget here
+            for req, g, need, adm, nsteps, tg in retiring:
+                ts = self.clock()
+                up = eng.finish(g, self.keep)
+                self.host_s["retire"] += self.clock() - ts
+                results.append(Result(req.id, req.kind, req.cells, req.arrival, adm, self.clock() - t0,
+                                      nsteps, tg, up))
+                used -= need
+            retiring = []
             now = self.clock() - t0
             while pending and pending[0].arrival <= now:
-                waiting.append(pending.popleft())
+                req = pending.popleft()
+                if hasattr(eng, "announce"):
+                    eng.announce(req)
+                waiting.append(req)
             while waiting and len(active) < self.max_active:
                 req = waiting[0]
                 need = eng.bytes_needed(req)
@@ -205,7 +266,9 @@ class SolveServer:
                 if used + need > self.budget:
                     break  # first come, first served: wait for memory to free up
                 waiting.popleft()
+                ts = self.clock()
                 g = eng.prepare(req)
+                self.host_s["prepare"] += self.clock() - ts
                 active.append([req, g, need, self.clock() - t0])
                 new_clock.append((0.0, req.final_time))
                 used += need
@@ -213,22 +276,22 @@ class SolveServer:
             self.peak_bytes = max(self.peak_bytes, used)
             self.peak_active = max(self.peak_active, len(active))
             if batch is not None:
+                ts = self.clock()
                 t, steps, act = eng.clocks(batch)  # waits for the round
-                done_now = self.clock() - t0
+                self.host_s["wait"] += self.clock() - ts
                 keep_rows, keep_clock = [], []
                 for k, row in enumerate(active):
                     if k < len(act) and not act[k]:
-                        req, g, need, adm = row
-                        up = eng.finish(g, self.keep)
-                        results.append(Result(req.id, req.kind, req.cells, req.arrival, adm, done_now,
-                                              int(steps[k]), float(t[k]), up))
-                        used -= need
+                        if hasattr(eng, "detach"):
+                            eng.detach(row[1])
+                        retiring.append(row + [int(steps[k]), float(t[k])])
                         changed = True
                     else:
                         keep_rows.append(row)
                         keep_clock.append(new_clock[k])
                 active, new_clock = keep_rows, keep_clock
             if changed:
+                ts = self.clock()
                 if batch is not None:
                     eng.close_batch(batch)
                     batch = None
@@ -237,7 +300,8 @@ class SolveServer:
                     new_clock = [None] * len(active)
                     self.rebuilds += 1
                 changed = False
-            if not active and pending and not waiting:
+                self.host_s["rebuild"] += self.clock() - ts
+            if not active and not retiring and pending and not waiting:
                 wait = pending[0].arrival - (self.clock() - t0)
                 if wait > 0:
                     self.sleep(wait)
@@ -269,11 +333,13 @@ def main(argv=None):
     args = ap.parse_args(argv)
     reqs = make_stream(args.requests, args.seed, args.rate, args.michel_final_time,
                        riemann_cells=(128, args.max_riemann_cells), michel_cells=(512, args.max_michel_cells))
-    srv = SolveServer(GpuEngine(args.precision), steps_per_round=args.steps_per_round)
+    eng = GpuEngine(args.precision)
+    srv = SolveServer(eng, steps_per_round=args.steps_per_round)
     res = srv.run(reqs)
+    eng.close()
     out = summarize(res)
     out.update(peak_active=srv.peak_active, peak_bytes=srv.peak_bytes, rounds=srv.rounds, rebuilds=srv.rebuilds,
-               budget_bytes=srv.budget, precision=args.precision)
+               budget_bytes=srv.budget, precision=args.precision, host_s=srv.host_s, engine_host_s=eng.host_s)
     print(json.dumps(out))
 
 

@@ -31,6 +31,7 @@ def test_results_equal_solo_runs(precision):
     budget = sum(sorted(eng.bytes_needed(r) for r in reqs)[-6:])  # about six grids at a time
     srv = SolveServer(eng, budget_bytes=budget, steps_per_round=8, keep_results=True)
     res = srv.run(reqs)
+    eng.close()
     assert len(res) == len(reqs) and srv.peak_bytes <= budget
     assert srv.rebuilds > 1 and 1 < srv.peak_active < len(reqs)
     for r, q in zip(res, reqs):
