@@ -1,9 +1,9 @@
 // flux.cuh -- face fluxes of one direction as two lean kernels.
 //
-//   k_recon<DIR, REC>   one thread per (face, variable): loads the variable's stencil
-//                       (boundary fill evaluated on load), selects the branch of
-//                       reconstruct_1d_core (reconstruction.f90:318-645) from the density
-//                       and pressure stencils, writes q_L, q_R with the positivity floors
+//   k_recon<DIR, REC>   one thread per face: selects the branch of reconstruct_1d_core
+//                       (reconstruction.f90:318-645) from the density and pressure
+//                       stencils, then per variable loads the stencil (boundary fill
+//                       evaluated on load) and writes q_L, q_R with the positivity floors
 //                       (reconstruction.f90:647-655).
 //   k_riemann<DIR, RS>  one thread per face: resolve_riemann_problem (fluxes.f90:56) on
 //                       the reconstructed states, zero flux on degenerate faces
@@ -151,22 +151,24 @@ __device__ __forceinline__ void recon_one(int br, int lim, const R (&s)[6], R &q
 // Batched launches: block b works on grid map[b].grid, tile map[b].first / blockDim.x.
 // Q layout per grid: Q[(side*5 + v) * nfaces + f], side 0 = q_L, 1 = q_R
 // Resident blocks per SM the register allocation must allow (256-thread recon blocks,
-// 128-thread Riemann blocks).  Both kernels stall on dependent FP64 chains, so occupancy
-// pays more than the few registers it costs: measured on the batched 2.5D torus and the
-// 3D torus, 5 recon blocks (51 registers) and 8 Riemann blocks (64 registers) are fastest.
+// 128-thread Riemann blocks), measured on the batched 2.5D torus and the 3D torus: recon
+// 4 (64 registers); Riemann 8 for HLLE (64 registers), HLLC 4 in FP64 (128 registers)
+// and 6 in FP32 (80): HLLC's larger state spills at 64.
 #ifndef GRHD_RECON_MIN_BLOCKS
-#define GRHD_RECON_MIN_BLOCKS 5
+#define GRHD_RECON_MIN_BLOCKS 4
 #endif
-#ifndef GRHD_RIEMANN_MIN_BLOCKS
-#define GRHD_RIEMANN_MIN_BLOCKS 8
-#endif
+template <int RS, class R>
+constexpr int riemann_min_blocks() { return RS == RS_HLLC ? (sizeof(R) == sizeof(double) ? 4 : 6) : 8; }
+// One thread per face reconstructs all five variables (rolled variable loop): the set-up
+// of a work item (block map, descriptor, tile decode, window check, the sensor's density
+// and pressure windows and branch) is paid once per face.  Measured against one thread
+// per (face, variable): FP64 2.5D torus batch +2 %, 3D torus (MP5 + sensor) +24 %.
 template <int DIR, int REC, class R, class PT>
 __global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;
   const long long nf = n_faces<DIR>(G);
-  const int v = blockIdx.y;
   unsigned nI, nJ, nK, a, b, c;
   face_space<DIR>(G, nI, nJ, nK);
   if (!tile_item<8>(G.tiles[TILE_RECON + DIR - 1], (unsigned)bm.first >> 8, threadIdx.x, nI, nJ, nK, a, b, c) ||
@@ -175,12 +177,10 @@ __global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const Grid
   const long long f = (long long)a + (long long)nI * ((long long)b + (long long)nJ * c);
   const PT *__restrict__ Pin = (const PT *)G.P;
   R *__restrict__ Q = (R *)G.Q;
-  unsigned long long *cnt = G.cnt;
   const FaceIndex x = face_at<DIR>(G, a, b, c);
   const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
   int lo, hi;
   stencil_range(REC, P.sensor, lo, hi);
-  // a stencil entirely inside the grid reads P directly at a fixed stride along DIR
   const bool inside = x.face - 2 + lo >= 1 && x.face - 2 + hi <= n;
   const long long stride = DIR == 1 ? 1LL : (DIR == 2 ? (long long)G.nx : (long long)G.nx * G.ny);
   long long base = 0;
@@ -192,36 +192,34 @@ __global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const Grid
     return inside ? R((double)GRHD_LDP(&Pin[w * G.pplane + base + m * stride]))
                   : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, w));
   };
-  R s[6];
-#pragma unroll
-  for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ld(v, m) : R(0);
   int br = BR_GODUNOV;
   if (REC != REC_GODUNOV) {
     R rho[5], pr[5];
-    if (P.sensor) {
 #pragma unroll
-      for (int m = 0; m < 5; ++m) {
-        rho[m] = v == EQ_DE ? s[m] : ld(EQ_DE, m);
-        pr[m] = v == EQ_PR ? s[m] : ld(EQ_PR, m);
-      }
-    } else {
-#pragma unroll
-      for (int m = 0; m < 5; ++m) { rho[m] = R(0); pr[m] = R(0); }
+    for (int m = 0; m < 5; ++m) {
+      rho[m] = P.sensor ? ld(EQ_DE, m) : R(0);
+      pr[m] = P.sensor ? ld(EQ_PR, m) : R(0);
     }
     br = branch_of<REC>(P, rho, pr, x.face, n, DIR);
   }
-  R qL, qR;
-  recon_one<REC>(br, P.lim, s, qL, qR);
   unsigned clamps = 0;
-  if (v == EQ_DE || v == EQ_PR) {  // reconstruction.f90:647-655
-    const R fl = v == EQ_DE ? R(P.rho_floor) : R(P.p_floor);
-    clamps = (unsigned)!(qL >= fl) + (unsigned)!(qR >= fl);
-    qL = rmax(qL, fl);
-    qR = rmax(qR, fl);
+#pragma unroll 1
+  for (int v = 0; v < NEQ; ++v) {
+    R s[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ld(v, m) : R(0);
+    R qL, qR;
+    recon_one<REC>(br, P.lim, s, qL, qR);
+    if (v == EQ_DE || v == EQ_PR) {  // reconstruction.f90:647-655
+      const R fl = v == EQ_DE ? R(P.rho_floor) : R(P.p_floor);
+      clamps += (unsigned)!(qL >= fl) + (unsigned)!(qR >= fl);
+      qL = rmax(qL, fl);
+      qR = rmax(qR, fl);
+    }
+    Q[(long long)v * nf + f] = qL;
+    Q[(long long)(5 + v) * nf + f] = qR;
   }
-  Q[(long long)v * nf + f] = qL;
-  Q[(long long)(5 + v) * nf + f] = qR;
-  count_add(cnt, CNT_RECON_CLAMP, clamps);
+  count_add(G.cnt, CNT_RECON_CLAMP, clamps);
 }
 
 // ------------------------------------------------------------------------------------
@@ -345,7 +343,7 @@ __global__ void __launch_bounds__(FLUX_BS, flux_min_blocks<R>())
 }
 
 template <int DIR, int RS, class R>
-__global__ void __launch_bounds__(128, GRHD_RIEMANN_MIN_BLOCKS) k_riemann(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+__global__ void __launch_bounds__(128, riemann_min_blocks<RS, R>()) k_riemann(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;

@@ -5,18 +5,19 @@
 #pragma once
 
 #include "flux.cuh"
+#include "flux_launch.h"
 
 namespace grhd {
 
 template <int DIR, class R, class PT>
 inline void recon_dir(int rec, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
-  const dim3 grid((unsigned)nblocks, 5);
+  const unsigned nb = (unsigned)nblocks;
   switch (rec) {
-    case REC_GODUNOV: k_recon<DIR, REC_GODUNOV, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
-    case REC_TVD: k_recon<DIR, REC_TVD, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
-    case REC_WENO3: k_recon<DIR, REC_WENO3, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
-    case REC_MP5: k_recon<DIR, REC_MP5, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
-    default: k_recon<DIR, REC_WENO5, R, PT><<<grid, 256, 0, s>>>(grids, map); break;
+    case REC_GODUNOV: k_recon<DIR, REC_GODUNOV, R, PT><<<nb, RECON_BS, 0, s>>>(grids, map); break;
+    case REC_TVD: k_recon<DIR, REC_TVD, R, PT><<<nb, RECON_BS, 0, s>>>(grids, map); break;
+    case REC_WENO3: k_recon<DIR, REC_WENO3, R, PT><<<nb, RECON_BS, 0, s>>>(grids, map); break;
+    case REC_MP5: k_recon<DIR, REC_MP5, R, PT><<<nb, RECON_BS, 0, s>>>(grids, map); break;
+    default: k_recon<DIR, REC_WENO5, R, PT><<<nb, RECON_BS, 0, s>>>(grids, map); break;
   }
 }
 
