@@ -95,66 +95,92 @@ __device__ __forceinline__ void c2p_count(unsigned long long *cnt, unsigned fl) 
 // Batched: block b works on grid map[b].grid, cell tile map[b].first / 128.
 // Resident 128-thread blocks per SM the register allocation must allow.  The kernel waits
 // on dependent FP64 chains (con2prim) and scattered table loads, so more warps in flight
-// pay for a few spilled registers: measured on the 2.5D torus batch, 8 blocks (64
-// registers) is fastest for FP64 and 6 (80 registers) for the mixed policy.
+// pay for a few spilled registers: measured on the 2.5D and 3D torus batches, 8 blocks
+// (64 registers) is fastest for FP64 and 6 (80 registers; 7 and 8 measured slower) for
+// the mixed policy.
 template <class PT>
 constexpr int cell_min_blocks() { return sizeof(PT) == sizeof(double) ? 8 : 6; }
 
+// Where cell_core reads a cell's streamed inputs: the primitives, the two faces of each
+// active direction, and up, u.  DirectIn loads them from global memory where they are
+// used; StagedIn (below) has them copied into shared memory ahead of use.
+struct CellIndex {
+  long long c;     // cell index in the state planes
+  unsigned i, j, k;
+};
+__device__ __forceinline__ CellIndex cell_index_of(const GridDev &G, unsigned ia, unsigned jb, unsigned kc) {
+  return CellIndex{(long long)ia + (long long)G.nx * ((long long)jb + (long long)G.ny * kc), ia, jb, kc};
+}
+// lower face of the cell along direction d (0..2), the face count, the upper face's offset
+__device__ __forceinline__ long long face_lo(const GridDev &G, const CellIndex &x, int d) {
+  if (d == 0) return x.i + (long long)(G.nx + 1) * (x.j + (long long)G.ny * x.k);
+  if (d == 1) return x.i + (long long)G.nx * (x.j + (long long)(G.ny + 1) * x.k);
+  return x.i + (long long)G.nx * (x.j + (long long)G.ny * x.k);
+}
+__device__ __forceinline__ long long face_n(const GridDev &G, int d) {
+  if (d == 0) return (long long)(G.nx + 1) * G.ny * G.nz;
+  if (d == 1) return (long long)G.nx * (G.ny + 1) * G.nz;
+  return (long long)G.nx * G.ny * (G.nz + 1);
+}
+__device__ __forceinline__ long long face_up(const GridDev &G, int d) {
+  return d == 0 ? 1LL : (d == 1 ? (long long)G.nx : (long long)G.nx * G.ny);
+}
+
+template <class R, class PT>
+struct DirectIn {
+  const GridDev &G;
+  const CellIndex &x;
+  __device__ __forceinline__ void wait_prims() const {}
+  __device__ __forceinline__ void wait_fluxes() const {}
+  __device__ __forceinline__ void wait_state() const {}
+  __device__ __forceinline__ double prim(int v) const { return (double)((const PT *)G.P)[v * G.pplane + x.c]; }
+  __device__ __forceinline__ R flux(int d, int upper, int v) const {
+    return ((const R *)G.F[d])[v * face_n(G, d) + face_lo(G, x, d) + (upper ? face_up(G, d) : 0)];
+  }
+  __device__ __forceinline__ double up(int v) const { return G.UP[v * G.pplane + x.c]; }
+  __device__ __forceinline__ double u(int v) const { return G.U[v * G.pplane + x.c]; }
+};
+
 // One cell (ia, jb, kc), 0-based.  MODE 0 writes the RHS; 1..3 run the RK stage.  The
 // mode is a run-time argument so a persistent kernel needs one copy of the code; the
-// stage kernels pass a constant and the compiler folds it.
-template <class R, class PT>
-__device__ __forceinline__ void cell_item(const GridDev &G, unsigned ia, unsigned jb, unsigned kc, const int MODE) {
-  const long long c = (long long)ia + (long long)G.nx * ((long long)jb + (long long)G.ny * kc);
+// stage kernels pass a constant and the compiler folds it.  The clock has been checked
+// by the caller (dt: the grid's step, 0 in MODE 0).
+template <class R, class PT, class In>
+__device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigned jb, const CellIndex &x, const int MODE,
+                                          double dt, const In &in) {
+  const long long c = x.c;
   const Phys P = G.phys;
   PT *__restrict__ Pio = (PT *)G.P;
-  const R *__restrict__ Fx = (const R *)G.F[0];
-  const R *__restrict__ Fy = (const R *)G.F[1];
-  const R *__restrict__ Fz = (const R *)G.F[2];
   double *__restrict__ U = G.U;
   double *__restrict__ UP = G.UP;
   double *__restrict__ rhs_out = G.RHS;
   const double dx = G.dx, dy = G.dy, dz = G.dz;
-  double dt = 0.0;
-  if (MODE != 0) {
-    const GridClock ck = *G.clock;
-    if (clock_skip(ck)) return;
-    dt = clock_dt(ck);
-  }
   unsigned long long *cnt = G.cnt;
-  const int i0 = (int)ia, j0 = (int)jb, k0 = (int)kc;
-  const long long ij = i0 + (long long)G.nx * j0;
+  const long long ij = (long long)ia + (long long)G.nx * jb;
+  in.wait_prims();
   double q[NEQ];
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v) q[v] = (double)Pio[v * G.pplane + c];
+  for (int v = 0; v < NEQ; ++v) q[v] = in.prim(v);
   R src[NEQ];
   sources<R>(G, P, ij, q, src);
+  in.wait_fluxes();
   double rhs[NEQ];
-  {
-    const long long nfx = (long long)(G.nx + 1) * G.ny * G.nz;
-    const long long fx = i0 + (long long)(G.nx + 1) * (j0 + (long long)G.ny * k0);
 #pragma unroll
-    for (int v = 0; v < NEQ; ++v) {
-      const R a = Fx[v * nfx + fx + 1], b = Fx[v * nfx + fx];
-      rhs[v] = (double)(-(a - b) / R(dx) + src[v]);
-    }
+  for (int v = 0; v < NEQ; ++v) {
+    const R a = in.flux(0, 1, v), b = in.flux(0, 0, v);
+    rhs[v] = (double)(-(a - b) / R(dx) + src[v]);
   }
   if (G.ny > 1) {
-    const long long nfy = (long long)G.nx * (G.ny + 1) * G.nz;
-    const long long fy = i0 + (long long)G.nx * (j0 + (long long)(G.ny + 1) * k0);
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
-      const R a = Fy[v * nfy + fy + G.nx], b = Fy[v * nfy + fy];
+      const R a = in.flux(1, 1, v), b = in.flux(1, 0, v);
       rhs[v] = (double)(R(rhs[v]) - (a - b) / R(dy));
     }
   }
   if (G.nz > 1) {
-    const long long nfz = (long long)G.nx * G.ny * (G.nz + 1);
-    const long long fz = i0 + (long long)G.nx * (j0 + (long long)G.ny * k0);
-    const long long st = (long long)G.nx * G.ny;
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
-      const R a = Fz[v * nfz + fz + st], b = Fz[v * nfz + fz];
+      const R a = in.flux(2, 1, v), b = in.flux(2, 0, v);
       rhs[v] = (double)(R(rhs[v]) - (a - b) / R(dz));
     }
   }
@@ -163,18 +189,19 @@ __device__ __forceinline__ void cell_item(const GridDev &G, unsigned ia, unsigne
     for (int v = 0; v < NEQ; ++v) rhs_out[v * G.pplane + c] = rhs[v];
     return;
   }
+  in.wait_state();
   double cs[NEQ];
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) {
-    const double up = UP[v * G.pplane + c];
+    const double up = in.up(v);
     double nv;
     if (MODE == 1) {
       U[v * G.pplane + c] = up;  // u = up (grhd2.f90:232)
       nv = up + rhs[v] * dt;
     } else if (MODE == 2) {
-      nv = 0.75 * U[v * G.pplane + c] + 0.25 * (up + rhs[v] * dt);
+      nv = 0.75 * in.u(v) + 0.25 * (up + rhs[v] * dt);
     } else {
-      nv = (U[v * G.pplane + c] + 2.0 * (up + rhs[v] * dt)) / 3.0;
+      nv = (in.u(v) + 2.0 * (up + rhs[v] * dt)) / 3.0;
     }
     cs[v] = nv;
   }
@@ -197,16 +224,126 @@ __device__ __forceinline__ void cell_item(const GridDev &G, unsigned ia, unsigne
   c2p_count(cnt, fl);
 }
 
+template <class R, class PT>
+__device__ __forceinline__ void cell_item(const GridDev &G, unsigned ia, unsigned jb, unsigned kc, const int MODE) {
+  double dt = 0.0;
+  if (MODE != 0) {
+    const GridClock ck = *G.clock;
+    if (clock_skip(ck)) return;
+    dt = clock_dt(ck);
+  }
+  const CellIndex x = cell_index_of(G, ia, jb, kc);
+  cell_core<R, PT>(G, ia, jb, x, MODE, dt, DirectIn<R, PT>{G, x});
+}
+
+// ---- staged inputs ------------------------------------------------------------------
+// Each thread copies its own cell's streamed inputs into shared memory with cp.async
+// (sm_80+ asynchronous global->shared copies; a thread waits for its own groups, so no
+// block barrier is needed) in three commit groups: primitives, face fluxes, then up and
+// u.  All the copies are in flight at once without holding registers, and the sources
+// (which need only the primitives and the metric tables) overlap the flux and RK-state
+// fetches.  Layout per block, structure of arrays over the block's threads:
+//   double up[NEQ][CELL_BS], u[NEQ][CELL_BS]; PT p[NEQ][CELL_BS];
+//   R f[2 * dirs][NEQ][CELL_BS]   (lower, upper face of each active direction)
+constexpr int CELL_BS_STAGE = 128;
+// Staging pays for the mixed policy (measured on the 2.5D and 3D torus batches: cell
+// update -7 %); the FP64 kernel is bound by its FP64 instruction stream and runs as fast
+// with direct loads and no shared memory limiting its resident blocks.
+template <class PT>
+__host__ __device__ constexpr bool cell_staged() { return sizeof(PT) == sizeof(float); }
+template <class R, class PT>
+__host__ __device__ constexpr size_t cell_stage_bytes(int dirs) {
+  return cell_staged<PT>()
+             ? (size_t)CELL_BS_STAGE * (2 * NEQ * sizeof(double) + NEQ * sizeof(PT) + 2 * dirs * NEQ * sizeof(R))
+             : 0;
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <class R, class PT>
+struct StagedIn {
+  const double *s_up, *s_u;
+  const PT *s_p;
+  const R *s_f;
+  int t, slot[3];
+  __device__ __forceinline__ StagedIn(const GridDev &G, const CellIndex &x, const int MODE, unsigned char *raw) {
+    t = threadIdx.x;
+    double *up = (double *)raw;
+    double *u = up + NEQ * CELL_BS_STAGE;
+    PT *p = (PT *)(u + NEQ * CELL_BS_STAGE);
+    R *f = (R *)(p + NEQ * CELL_BS_STAGE);
+    s_up = up; s_u = u; s_p = p; s_f = f;
+    slot[0] = 0;
+    slot[1] = 1;
+    slot[2] = G.ny > 1 ? 2 : 1;
+    const PT *Pg = (const PT *)G.P;
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) cp_async<sizeof(PT)>(&p[v * CELL_BS_STAGE + t], &Pg[v * G.pplane + x.c]);
+    cp_async_commit();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if ((d == 1 && G.ny == 1) || (d == 2 && G.nz == 1)) continue;
+      const R *Fg = (const R *)G.F[d];
+      const long long lo = face_lo(G, x, d), nf = face_n(G, d), off = face_up(G, d);
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) {
+        cp_async<sizeof(R)>(&f[((2 * slot[d]) * NEQ + v) * CELL_BS_STAGE + t], &Fg[v * nf + lo]);
+        cp_async<sizeof(R)>(&f[((2 * slot[d] + 1) * NEQ + v) * CELL_BS_STAGE + t], &Fg[v * nf + lo + off]);
+      }
+    }
+    cp_async_commit();
+    if (MODE != 0) {
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) cp_async<8>(&up[v * CELL_BS_STAGE + t], &G.UP[v * G.pplane + x.c]);
+      if (MODE >= 2) {
+#pragma unroll
+        for (int v = 0; v < NEQ; ++v) cp_async<8>(&u[v * CELL_BS_STAGE + t], &G.U[v * G.pplane + x.c]);
+      }
+    }
+    cp_async_commit();
+  }
+  __device__ __forceinline__ void wait_prims() const { cp_async_wait<2>(); }
+  __device__ __forceinline__ void wait_fluxes() const { cp_async_wait<1>(); }
+  __device__ __forceinline__ void wait_state() const { cp_async_wait<0>(); }
+  __device__ __forceinline__ double prim(int v) const { return (double)s_p[v * CELL_BS_STAGE + t]; }
+  __device__ __forceinline__ R flux(int d, int upper, int v) const {
+    return s_f[((2 * slot[d] + upper) * NEQ + v) * CELL_BS_STAGE + t];
+  }
+  __device__ __forceinline__ double up(int v) const { return s_up[v * CELL_BS_STAGE + t]; }
+  __device__ __forceinline__ double u(int v) const { return s_u[v * CELL_BS_STAGE + t]; }
+};
+
+// dirs: the most active directions of any grid of the launch (sizes the dynamic shared
+// memory, cell_stage_bytes<R, PT>(dirs) bytes)
 template <int MODE, class R, class PT>
-__global__ void __launch_bounds__(128, cell_min_blocks<PT>())
+__global__ void __launch_bounds__(CELL_BS_STAGE, cell_min_blocks<PT>())
     k_cell_update(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+  extern __shared__ __align__(16) unsigned char cell_stage[];
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   unsigned ia, jb, kc;
   if (!tile_item<7>(G.tiles[TILE_CELL], (unsigned)bm.first >> 7, threadIdx.x, (unsigned)G.nx, (unsigned)G.ny,
                     (unsigned)G.nz, ia, jb, kc))
     return;
-  cell_item<R, PT>(G, ia, jb, kc, MODE);
+  if (!cell_staged<PT>()) {
+    cell_item<R, PT>(G, ia, jb, kc, MODE);
+    return;
+  }
+  double dt = 0.0;
+  if (MODE != 0) {
+    const GridClock ck = *G.clock;
+    if (clock_skip(ck)) return;
+    dt = clock_dt(ck);
+  }
+  const CellIndex x = cell_index_of(G, ia, jb, kc);
+  const StagedIn<R, PT> in(G, x, MODE, cell_stage);
+  cell_core<R, PT>(G, ia, jb, x, MODE, dt, in);
 }
 
 }  // namespace grhd

@@ -2,5 +2,5 @@
 #include "cell_launch.cuh"
 
 namespace grhd {
-template void launch_cell<float, float>(int, const GridDev *, const BlockMap *, int, cudaStream_t);
+template void launch_cell<float, float>(int, const GridDev *, const BlockMap *, int, int, cudaStream_t);
 }  // namespace grhd

@@ -35,9 +35,9 @@ GRHD_FLUX_EXTERN(3, float, float)
 
 // stage cell kernel (cell_fp64.cu / cell_fp32.cu): mode 0 RHS only, 1..3 RK stages
 template <class R, class PT>
-void launch_cell(int mode, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
-extern template void launch_cell<double, double>(int, const GridDev *, const BlockMap *, int, cudaStream_t);
-extern template void launch_cell<float, float>(int, const GridDev *, const BlockMap *, int, cudaStream_t);
+void launch_cell(int mode, const GridDev *grids, const BlockMap *map, int nblocks, int dirs, cudaStream_t s);
+extern template void launch_cell<double, double>(int, const GridDev *, const BlockMap *, int, int, cudaStream_t);
+extern template void launch_cell<float, float>(int, const GridDev *, const BlockMap *, int, int, cudaStream_t);
 
 // persistent step kernel (persistent.cuh): one contiguous range of items of a phase --
 // the faces of one direction of one grid (dir 1..3) or the cells of one grid (dir 0)

@@ -164,6 +164,7 @@ struct Group {
   int nseg_face = 0, nseg_cell = 0;
   long long n_face = 0, n_cell = 0;
   int max_blocks = 0;  // resident blocks of the group's persistent instantiation
+  int cell_dirs = 1;   // the most active directions of a member grid (cell kernel staging)
 };
 
 struct FluxChoice {
@@ -362,6 +363,7 @@ int build_batch(grhd2_gpu_batch *b) {
       grp = &b->groups.back();
     }
     grp->members.push_back(g);
+    grp->cell_dirs = std::max(grp->cell_dirs, 1 + (h->cfg.ny > 1 ? 1 : 0) + (h->cfg.nz > 1 ? 1 : 0));
   }
   // flux variant and tile per scheme group and direction; the tiles go into the batch's
   // copies of the descriptors
@@ -465,7 +467,7 @@ int enqueue_fluxes(grhd2_gpu_batch *b, const Group &grp, cudaStream_t st) {
 template <int MODE, class R, class PT>
 int enqueue_cells(grhd2_gpu_batch *b, const Group &grp, cudaStream_t st) {
   if (grp.nb[K_CELL] <= 0) return 0;
-  launch_cell<R, PT>(MODE, b->d_grids, grp.d_map + grp.off[K_CELL], grp.nb[K_CELL], st);
+  launch_cell<R, PT>(MODE, b->d_grids, grp.d_map + grp.off[K_CELL], grp.nb[K_CELL], grp.cell_dirs, st);
   return blaunch_check(b, MODE == 0 ? "cell_rhs" : "cell_update");
 }
 
