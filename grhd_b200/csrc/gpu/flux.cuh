@@ -222,6 +222,74 @@ __global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const Grid
   count_add(G.cnt, CNT_RECON_CLAMP, clamps);
 }
 
+// The same reconstruction with one thread per (face, variable), blockIdx.y = variable:
+// five times the threads of k_recon, for launches too small to fill the GPU with one
+// thread per face (a single 2.5D grid: 400x1x200 has 80k faces per direction).  Its
+// launch bound (5 blocks, 48 registers) was measured on such launches.
+template <int DIR, int REC, class R, class PT>
+__global__ void __launch_bounds__(256, 5) k_recon_var(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+  const BlockMap bm = map[blockIdx.x];
+  const GridDev &G = grids[bm.grid];
+  const Phys P = G.phys;
+  const long long nf = n_faces<DIR>(G);
+  const int v = blockIdx.y;
+  unsigned nI, nJ, nK, a, b, c;
+  face_space<DIR>(G, nI, nJ, nK);
+  if (!tile_item<8>(G.tiles[TILE_RECON + DIR - 1], (unsigned)bm.first >> 8, threadIdx.x, nI, nJ, nK, a, b, c) ||
+      clock_skip(*G.clock))
+    return;
+  const long long f = (long long)a + (long long)nI * ((long long)b + (long long)nJ * c);
+  const PT *__restrict__ Pin = (const PT *)G.P;
+  R *__restrict__ Q = (R *)G.Q;
+  unsigned long long *cnt = G.cnt;
+  const FaceIndex x = face_at<DIR>(G, a, b, c);
+  const int n = DIR == 1 ? G.nx : (DIR == 2 ? G.ny : G.nz);
+  int lo, hi;
+  stencil_range(REC, P.sensor, lo, hi);
+  // a stencil entirely inside the grid reads P directly at a fixed stride along DIR
+  const bool inside = x.face - 2 + lo >= 1 && x.face - 2 + hi <= n;
+  const long long stride = DIR == 1 ? 1LL : (DIR == 2 ? (long long)G.nx : (long long)G.nx * G.ny);
+  long long base = 0;
+  if (inside) {
+    const int c0 = x.face - 2 + lo;
+    base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
+  }
+  auto ld = [&](int w, int m) -> R {
+    return inside ? R((double)GRHD_LDP(&Pin[w * G.pplane + base + m * stride]))
+                  : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, w));
+  };
+  R s[6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ld(v, m) : R(0);
+  int br = BR_GODUNOV;
+  if (REC != REC_GODUNOV) {
+    R rho[5], pr[5];
+    if (P.sensor) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        rho[m] = v == EQ_DE ? s[m] : ld(EQ_DE, m);
+        pr[m] = v == EQ_PR ? s[m] : ld(EQ_PR, m);
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) { rho[m] = R(0); pr[m] = R(0); }
+    }
+    br = branch_of<REC>(P, rho, pr, x.face, n, DIR);
+  }
+  R qL, qR;
+  recon_one<REC>(br, P.lim, s, qL, qR);
+  unsigned clamps = 0;
+  if (v == EQ_DE || v == EQ_PR) {  // reconstruction.f90:647-655
+    const R fl = v == EQ_DE ? R(P.rho_floor) : R(P.p_floor);
+    clamps = (unsigned)!(qL >= fl) + (unsigned)!(qR >= fl);
+    qL = rmax(qL, fl);
+    qR = rmax(qR, fl);
+  }
+  Q[(long long)v * nf + f] = qL;
+  Q[(long long)(5 + v) * nf + f] = qR;
+  count_add(cnt, CNT_RECON_CLAMP, clamps);
+}
+
 // ------------------------------------------------------------------------------------
 // Fused alternative: one thread per face reconstructs all five variables and solves the
 // Riemann problem, so q_L, q_R never leave the SM.  Same arithmetic as k_recon + k_riemann

@@ -10,8 +10,19 @@
 namespace grhd {
 
 template <int DIR, class R, class PT>
-inline void recon_dir(int rec, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
+inline void recon_dir(int rec, bool per_variable, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
   const unsigned nb = (unsigned)nblocks;
+  if (per_variable) {
+    const dim3 grid(nb, 5);
+    switch (rec) {
+      case REC_GODUNOV: k_recon_var<DIR, REC_GODUNOV, R, PT><<<grid, RECON_BS, 0, s>>>(grids, map); break;
+      case REC_TVD: k_recon_var<DIR, REC_TVD, R, PT><<<grid, RECON_BS, 0, s>>>(grids, map); break;
+      case REC_WENO3: k_recon_var<DIR, REC_WENO3, R, PT><<<grid, RECON_BS, 0, s>>>(grids, map); break;
+      case REC_MP5: k_recon_var<DIR, REC_MP5, R, PT><<<grid, RECON_BS, 0, s>>>(grids, map); break;
+      default: k_recon_var<DIR, REC_WENO5, R, PT><<<grid, RECON_BS, 0, s>>>(grids, map); break;
+    }
+    return;
+  }
   switch (rec) {
     case REC_GODUNOV: k_recon<DIR, REC_GODUNOV, R, PT><<<nb, RECON_BS, 0, s>>>(grids, map); break;
     case REC_TVD: k_recon<DIR, REC_TVD, R, PT><<<nb, RECON_BS, 0, s>>>(grids, map); break;
@@ -22,11 +33,12 @@ inline void recon_dir(int rec, const GridDev *grids, const BlockMap *map, int nb
 }
 
 template <class R, class PT>
-void launch_recon(int dir, int rec, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s) {
+void launch_recon(int dir, int rec, bool per_variable, const GridDev *grids, const BlockMap *map, int nblocks,
+                  cudaStream_t s) {
   if (nblocks <= 0) return;
-  if (dir == 1) recon_dir<1, R, PT>(rec, grids, map, nblocks, s);
-  else if (dir == 2) recon_dir<2, R, PT>(rec, grids, map, nblocks, s);
-  else recon_dir<3, R, PT>(rec, grids, map, nblocks, s);
+  if (dir == 1) recon_dir<1, R, PT>(rec, per_variable, grids, map, nblocks, s);
+  else if (dir == 2) recon_dir<2, R, PT>(rec, per_variable, grids, map, nblocks, s);
+  else recon_dir<3, R, PT>(rec, per_variable, grids, map, nblocks, s);
 }
 
 template <class R>

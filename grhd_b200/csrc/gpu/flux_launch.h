@@ -16,7 +16,7 @@ constexpr int CELL_BS = 128;
 constexpr int FUSED_FLUX_BS = 128;  // k_flux (flux.cuh FLUX_BS)
 
 template <class R, class PT>
-void launch_recon(int dir, int rec, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
+void launch_recon(int dir, int rec, bool per_variable, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
 template <class R>
 void launch_riemann(int dir, int rs, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
 
@@ -77,8 +77,8 @@ inline void launch_flux(int dir, int rec, int rs, const GridDev *grids, const Bl
   else launch_flux_dir<3, R, PT>(rec, rs, grids, map, nblocks, s);
 }
 
-extern template void launch_recon<double, double>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
-extern template void launch_recon<float, float>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
+extern template void launch_recon<double, double>(int, int, bool, const GridDev *, const BlockMap *, int, cudaStream_t);
+extern template void launch_recon<float, float>(int, int, bool, const GridDev *, const BlockMap *, int, cudaStream_t);
 extern template void launch_riemann<double>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
 extern template void launch_riemann<float>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
 

@@ -325,6 +325,7 @@ TuneKey tune_key(const Group &grp, const std::vector<GridDev> &hg, int dir) {
 
 // default without tuning: the split kernels (recon at high occupancy, lean Riemann)
 constexpr int DEFAULT_VARIANT = GRHD2_FLUX_SPLIT;
+constexpr long long SPLIT_VAR_BELOW_FACES = 4LL * 148 * 4 * RECON_BS;  // four waves of per-face blocks
 // Automatic step mode: the graph of stage kernels.  Measured on one B200 with 1024-cell 1D
 // grids, a graph replay takes 83-88 us per step and the persistent kernel 127-135 us: a
 // small grid is bound by the dependent arithmetic chain of one item per thread, not by
@@ -334,13 +335,17 @@ constexpr int DEFAULT_VARIANT = GRHD2_FLUX_SPLIT;
 FluxChoice choose_flux(const grhd2_gpu_batch *b, int gi, const Group &grp, const std::vector<GridDev> &hg, int dir) {
   auto f = b->forced.find({gi, dir});
   if (f != b->forced.end()) return f->second;
-  FluxChoice c{DEFAULT_VARIANT, DEFAULT_TX};
+  // untuned: one thread per (face, variable) for launches that one thread per face would
+  // leave short of the resident threads of the GPU
+  long long faces = 0;
+  for (int g : grp.members) faces += face_count(hg[g], dir);
+  FluxChoice c{faces < SPLIT_VAR_BELOW_FACES ? GRHD2_FLUX_SPLIT_VAR : DEFAULT_VARIANT, DEFAULT_TX};
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune.find(tune_key(grp, hg, dir));
     if (it != g_tune.end()) c = it->second;
   }
-  if (b->variant_request == GRHD2_FLUX_SPLIT || b->variant_request == GRHD2_FLUX_FUSED) c.variant = b->variant_request;
+  if (b->variant_request != GRHD2_FLUX_AUTO) c.variant = b->variant_request;
   if (b->tile_request > 0) c.tx = b->tile_request;
   return c;
 }
@@ -447,7 +452,7 @@ int enqueue_dir(grhd2_gpu_batch *b, const Group &grp, int d, int variant, cudaSt
     return 0;
   }
   if (grp.nb[kr] > 0) {
-    launch_recon<R, PT>(d, grp.rec, b->d_grids, grp.d_map + grp.off[kr], grp.nb[kr], st);
+    launch_recon<R, PT>(d, grp.rec, variant == GRHD2_FLUX_SPLIT_VAR, b->d_grids, grp.d_map + grp.off[kr], grp.nb[kr], st);
     if (int rc = blaunch_check(b, KIND_NAME[kr])) return rc;
   }
   if (grp.nb[ks] > 0) {
@@ -1639,7 +1644,8 @@ int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *a
 
 int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant) {
   if (!b) return GRHD2_ERR_ARG;
-  if (variant != GRHD2_FLUX_AUTO && variant != GRHD2_FLUX_SPLIT && variant != GRHD2_FLUX_FUSED)
+  if (variant != GRHD2_FLUX_AUTO && variant != GRHD2_FLUX_SPLIT && variant != GRHD2_FLUX_FUSED &&
+      variant != GRHD2_FLUX_SPLIT_VAR)
     return bfail(b, GRHD2_ERR_ARG, "invalid flux variant %d", variant);
   BCUDA_TRY(b, cudaSetDevice(b->device));
   b->variant_request = variant;
@@ -1706,7 +1712,7 @@ int grhd2_gpu_batch_autotune(grhd2_gpu_batch *b, int reps, int *variants, int *t
       float best = 0.0f;
       FluxChoice best_c{DEFAULT_VARIANT, DEFAULT_TX};
       bool first = true;
-      for (int v : {GRHD2_FLUX_SPLIT, GRHD2_FLUX_FUSED}) {
+      for (int v : {GRHD2_FLUX_SPLIT, GRHD2_FLUX_SPLIT_VAR, GRHD2_FLUX_FUSED}) {
         for (unsigned tx : {32u, 64u, 128u}) {
           b->forced[{gi, d}] = FluxChoice{v, tx};
           if ((rc = build_batch(b))) break;

@@ -2,5 +2,5 @@
 #include "flux_launch.cuh"
 
 namespace grhd {
-template void launch_recon<float, float>(int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
+template void launch_recon<float, float>(int, int, bool, const GridDev *, const BlockMap *, int, cudaStream_t);
 }  // namespace grhd

@@ -126,7 +126,7 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--batch", type=int, default=1, help="replicas stepped as one batch")
     ap.add_argument("--graph", type=int, default=1, help="replay each step as a CUDA graph")
-    ap.add_argument("--flux", choices=["auto", "split", "fused", "tune"], default="tune",
+    ap.add_argument("--flux", choices=["auto", "split", "fused", "split_var", "tune"], default="tune",
                     help="face-flux kernel variant ('tune': time variants and tiles on this batch)")
     ap.add_argument("--tile", type=int, default=0, help="face-kernel tile extent along i (0: automatic)")
     ap.add_argument("--accuracy", action="store_true",

@@ -319,7 +319,7 @@ class GpuBatch:
         self._check(self.lib.grhd2_gpu_batch_get_clock(self._b, k, C.byref(t), C.byref(n), C.byref(a)))
         return t.value, n.value, bool(a.value)
 
-    FLUX_VARIANTS = {"auto": -1, "split": 0, "fused": 1}
+    FLUX_VARIANTS = {"auto": -1, "split": 0, "fused": 1, "split_var": 2}
 
     def set_flux_variant(self, variant: str):
         """'split' (recon + Riemann kernels), 'fused' (one kernel) or 'auto' (tuned/cached)."""

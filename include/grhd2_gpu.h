@@ -252,9 +252,11 @@ int grhd2_gpu_batch_profile_step(grhd2_gpu_batch *b, float *ms, const char **nam
  * the batch stream. */
 int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *active);
 /* Kernel variants of the face fluxes of one direction. */
-#define GRHD2_FLUX_AUTO -1  /* the autotuned choice for this shape if one is cached, else SPLIT */
-#define GRHD2_FLUX_SPLIT 0  /* reconstruction kernel (thread per face and variable) + Riemann kernel */
-#define GRHD2_FLUX_FUSED 1  /* one kernel, thread per face, interface states kept on chip */
+#define GRHD2_FLUX_AUTO -1      /* the autotuned choice for this shape if one is cached, else SPLIT_VAR for
+                                   launches under ~600k faces and SPLIT above */
+#define GRHD2_FLUX_SPLIT 0      /* reconstruction kernel (thread per face) + Riemann kernel */
+#define GRHD2_FLUX_FUSED 1      /* one kernel, thread per face, interface states kept on chip */
+#define GRHD2_FLUX_SPLIT_VAR 2  /* reconstruction kernel (thread per face and variable) + Riemann kernel */
 /* Use one variant for every scheme group and direction of the batch (or AUTO). */
 int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant);
 /* How a batch runs its steps. */
@@ -269,7 +271,7 @@ int grhd2_gpu_batch_step_mode(grhd2_gpu_batch *b);
  * the block along k (or j for grids without a k extent; the whole block along i for 1D
  * grids).  tx = 32, 64, 128 or 256; 0 restores the automatic choice. */
 int grhd2_gpu_batch_set_tile(grhd2_gpu_batch *b, int tx);
-/* Time every (variant, tile) pair -- SPLIT or FUSED, tx 32, 64 or 128 -- per scheme group
+/* Time every (variant, tile) pair -- SPLIT, SPLIT_VAR or FUSED, tx 32, 64 or 128 -- per scheme group
  * and active direction (reps launches after a warm-up, on the batch's current state) and
  * keep the fastest; the choice is also cached for later batches of the same precision,
  * scheme, solver, sensor, direction and size class.  The state and counters are left

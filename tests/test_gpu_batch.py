@@ -42,7 +42,8 @@ def _make(pb, stream, precision="fp64"):
 
 @pytest.mark.parametrize("graph,variant,tile,mode", [
     (True, "split", 0, "graph"), (False, "split", 128, "graph"), (True, "fused", 0, "graph"),
-    (False, "fused", 64, "graph"), (True, "split", 256, "graph"), (True, "split", 0, "persistent")])
+    (False, "fused", 64, "graph"), (True, "split", 256, "graph"), (True, "split", 0, "persistent"),
+    (True, "split_var", 0, "graph"), (False, "split_var", 64, "graph")])
 def test_batch_matches_oracle_per_grid(graph, variant, tile, mode):
     s = _stream()
     cases = _cases()
@@ -160,7 +161,7 @@ def test_batch_profile_names():
 
 
 def test_autotune_leaves_state_and_counters():
-    """Autotuning times both flux variants on the live state: afterwards the state and the
+    """Autotuning times the flux variants on the live state: afterwards the state and the
     counters are unchanged, and stepping with the tuned variants gives the solo result."""
     s = _stream()
     pbs = [torus_3d(nx=24, ny=12, nz=12), shock_tube(nx=200, rec="weno5", rs="hlle", sensor=True)]
@@ -178,7 +179,7 @@ def test_autotune_leaves_state_and_counters():
     before = [(g.download(want_p=False)[0], g.counters()) for g in grids]
     chosen = b.autotune(reps=2)
     assert len(chosen) == 3 + 1
-    assert all(v in ("split", "fused") and t in (32, 64, 128) for v, t in chosen)
+    assert all(v in ("split", "split_var", "fused") and t in (32, 64, 128) for v, t in chosen)
     for g, (up, cnt) in zip(grids, before):
         up2 = g.download(want_p=False)[0]
         assert np.array_equal(up, up2) and g.counters() == cnt
