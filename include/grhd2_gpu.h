@@ -102,7 +102,11 @@ typedef struct {
 typedef struct grhd2_gpu grhd2_gpu;
 
 /* Create a handle on the current CUDA device (allocates device state).  Replaces the
- * allocation half of allocate_and_grid (initialization.f90:84) for the hot-path arrays. */
+ * allocation half of allocate_and_grid (initialization.f90:84) for the hot-path arrays.
+ * Device buffers come from the device's stream-ordered memory pool (cudaMallocAsync on
+ * the handle's stream); grhd2_gpu_destroy returns them in stream order, and the pool keeps
+ * up to 8 GiB of released memory for later handles instead of handing it back to the
+ * driver, so creating and destroying handles never synchronises the device. */
 int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out);
 /* Upload the metric cache tables (precalculate_metric_cache, initialization.f90:265). */
 int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m);
