@@ -7,18 +7,28 @@
 
 namespace grhd {
 
+// Field fld of one (i,j) column of a centre table: from global memory, or from a block's
+// shared-memory slice of the table (SliceCol, below).
+template <class T>
+struct GlobalCol {
+  const T *__restrict__ C;
+  long long S, ij;
+  __device__ __forceinline__ T operator()(int fld) const { return __ldg(&C[fld * S + ij]); }
+};
+template <class T>
+__device__ __forceinline__ GlobalCol<T> global_col(const T *C, const GridDev &G, long long ij) {
+  return GlobalCol<T>{C, G.nij, ij};
+}
+
 // ------------------------------------------------------------------------------------
 // calc_sources (equations.f90:509-552) + calculate_stress_energy_tensor (metrics.f90:1251)
 // ------------------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ void sources(const GridDev &G, const Phys &P, long long ij, const double (&qd)[NEQ],
-                                        R (&src)[NEQ]) {
+template <class R, class Col>
+__device__ __forceinline__ void sources(const Phys &P, const Col &col, const double (&qd)[NEQ], R (&src)[NEQ]) {
 #pragma unroll
   for (int n = 0; n < NEQ; ++n) src[n] = R(0);
   if (P.srhd) return;
-  const R *__restrict__ C = centre_table<R>(G);
-  const long long S = G.nij;
-  auto ld = [&](int fld) { return R(__ldg(&C[fld * S + ij])); };
+  auto ld = [&](int fld) { return R(col(fld)); };
   const R alpha = ld(CF_ALPHA), sqg = ld(CF_SQG);
   FaceMetric<R> m;
   m.g11 = ld(CF_G11); m.g12 = ld(CF_G12); m.g13 = ld(CF_G13); m.g22 = ld(CF_G22); m.g23 = ld(CF_G23); m.g33 = ld(CF_G33);
@@ -62,16 +72,18 @@ __device__ __forceinline__ void sources(const GridDev &G, const Phys &P, long lo
   src[EQ_PR] = src[EQ_PR] * alpha;
 }
 
-__device__ __forceinline__ CellMetric load_cell_metric(const GridDev &G, long long ij) {
-  const double *__restrict__ C = G.centre;
-  const long long S = G.nij;
+template <class Col>
+__device__ __forceinline__ CellMetric load_cell_metric(const Col &C) {
   CellMetric m;
-  m.g11 = __ldg(&C[CF_G11 * S + ij]); m.g12 = __ldg(&C[CF_G12 * S + ij]); m.g13 = __ldg(&C[CF_G13 * S + ij]);
-  m.g22 = __ldg(&C[CF_G22 * S + ij]); m.g23 = __ldg(&C[CF_G23 * S + ij]); m.g33 = __ldg(&C[CF_G33 * S + ij]);
-  m.i11 = __ldg(&C[CF_I11 * S + ij]); m.i12 = __ldg(&C[CF_I12 * S + ij]); m.i13 = __ldg(&C[CF_I13 * S + ij]);
-  m.i22 = __ldg(&C[CF_I22 * S + ij]); m.i23 = __ldg(&C[CF_I23 * S + ij]); m.i33 = __ldg(&C[CF_I33 * S + ij]);
-  m.sqg = __ldg(&C[CF_SQG * S + ij]);
+  m.g11 = C(CF_G11); m.g12 = C(CF_G12); m.g13 = C(CF_G13);
+  m.g22 = C(CF_G22); m.g23 = C(CF_G23); m.g33 = C(CF_G33);
+  m.i11 = C(CF_I11); m.i12 = C(CF_I12); m.i13 = C(CF_I13);
+  m.i22 = C(CF_I22); m.i23 = C(CF_I23); m.i33 = C(CF_I33);
+  m.sqg = C(CF_SQG);
   return m;
+}
+__device__ __forceinline__ CellMetric load_cell_metric(const GridDev &G, long long ij) {
+  return load_cell_metric(global_col(G.centre, G, ij));
 }
 
 __device__ __forceinline__ void c2p_count(unsigned long long *cnt, unsigned fl) {
@@ -101,6 +113,48 @@ __device__ __forceinline__ void c2p_count(unsigned long long *cnt, unsigned fl) 
 template <class PT>
 constexpr int cell_min_blocks() { return sizeof(PT) == sizeof(double) ? 8 : 6; }
 
+// cp.async (sm_80+ asynchronous global->shared copy, cp-size 4, 8 or 16 bytes) and its
+// commit/wait; a thread waits for its own groups only.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// ---- the block's slice of a centre table ------------------------------------------------
+// Cell tiles of grids with a k extent are 32 cells along i x 4 along k, so the four warps
+// of a block share 32 (i,j) columns.  The block copies the NCF fields of those columns
+// into shared memory once ([NCF][32], with cp.async) and every thread reads its column
+// from there: ~70 table loads per cell that would otherwise go to L1/L2.
+constexpr int SLICE_COLS = 32;
+template <class T>
+__host__ __device__ constexpr size_t slice_bytes() { return (size_t)NCF * SLICE_COLS * sizeof(T); }
+template <class T>
+struct SliceCol {
+  const T *s;
+  unsigned lane;
+  __device__ __forceinline__ T operator()(int fld) const { return s[fld * SLICE_COLS + lane]; }
+};
+// whether the block's warps share their (i,j) columns (the tile layout above)
+__device__ __forceinline__ bool cell_tile_sliced(const GridDev &G) {
+  return G.nz > 1 && G.tiles[TILE_CELL].lx == 5 && G.tiles[TILE_CELL].ly == 0;
+}
+// every thread of the block takes part; columns beyond nx are left unset (no cell reads them)
+template <class T>
+__device__ __forceinline__ void stage_slice(T *slice, const T *C, const GridDev &G, unsigned i0, unsigned j) {
+  const long long S = G.nij;
+  const long long col0 = (long long)i0 + (long long)G.nx * j;
+  const unsigned ncols = min((unsigned)SLICE_COLS, (unsigned)G.nx - i0);
+  for (unsigned e = threadIdx.x; e < (unsigned)(NCF * SLICE_COLS); e += blockDim.x) {
+    const unsigned fld = e / SLICE_COLS, l = e % SLICE_COLS;
+    if (l < ncols) cp_async<sizeof(T)>(&slice[e], &C[fld * S + col0 + l]);
+  }
+  cp_async_commit();
+}
+
 // Where cell_core reads a cell's streamed inputs: the primitives, the two faces of each
 // active direction, and up, u.  DirectIn loads them from global memory where they are
 // used; StagedIn (below) has them copied into shared memory ahead of use.
@@ -126,13 +180,17 @@ __device__ __forceinline__ long long face_up(const GridDev &G, int d) {
   return d == 0 ? 1LL : (d == 1 ? (long long)G.nx : (long long)G.nx * G.ny);
 }
 
-template <class R, class PT>
+template <class R, class PT, class ColR = GlobalCol<R>, class Col64 = GlobalCol<double>>
 struct DirectIn {
   const GridDev &G;
   const CellIndex &x;
+  ColR cr;     // the centre table of arithmetic type R (sources)
+  Col64 c64;   // the FP64 centre table (con2prim metric)
   __device__ __forceinline__ void wait_prims() const {}
   __device__ __forceinline__ void wait_fluxes() const {}
   __device__ __forceinline__ void wait_state() const {}
+  __device__ __forceinline__ const ColR &table_r() const { return cr; }
+  __device__ __forceinline__ const Col64 &table64() const { return c64; }
   __device__ __forceinline__ double prim(int v) const { return (double)((const PT *)G.P)[v * G.pplane + x.c]; }
   __device__ __forceinline__ R flux(int d, int upper, int v) const {
     return ((const R *)G.F[d])[v * face_n(G, d) + face_lo(G, x, d) + (upper ? face_up(G, d) : 0)];
@@ -156,13 +214,12 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
   double *__restrict__ rhs_out = G.RHS;
   const double dx = G.dx, dy = G.dy, dz = G.dz;
   unsigned long long *cnt = G.cnt;
-  const long long ij = (long long)ia + (long long)G.nx * jb;
   in.wait_prims();
   double q[NEQ];
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) q[v] = in.prim(v);
   R src[NEQ];
-  sources<R>(G, P, ij, q, src);
+  sources<R>(P, in.table_r(), q, src);
   in.wait_fluxes();
   double rhs[NEQ];
 #pragma unroll
@@ -205,7 +262,7 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
     }
     cs[v] = nv;
   }
-  const CellMetric cm = load_cell_metric(G, ij);
+  const CellMetric cm = load_cell_metric(in.table64());
   // mixed policy: seed the root finder with the Lorentz factor of the current primitives
   double W_seed = 0.0;
   if (sizeof(PT) == sizeof(float)) {
@@ -233,7 +290,9 @@ __device__ __forceinline__ void cell_item(const GridDev &G, unsigned ia, unsigne
     dt = clock_dt(ck);
   }
   const CellIndex x = cell_index_of(G, ia, jb, kc);
-  cell_core<R, PT>(G, ia, jb, x, MODE, dt, DirectIn<R, PT>{G, x});
+  const long long ij = (long long)ia + (long long)G.nx * jb;
+  cell_core<R, PT>(G, ia, jb, x, MODE, dt,
+                   DirectIn<R, PT>{G, x, global_col(centre_table<R>(G), G, ij), global_col(G.centre, G, ij)});
 }
 
 // ---- staged inputs ------------------------------------------------------------------
@@ -257,22 +316,20 @@ __host__ __device__ constexpr size_t cell_stage_bytes(int dirs) {
              ? (size_t)CELL_BS_STAGE * (2 * NEQ * sizeof(double) + NEQ * sizeof(PT) + 2 * dirs * NEQ * sizeof(R))
              : 0;
 }
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <class R, class PT>
+template <class R, class PT, class ColR, class Col64>
 struct StagedIn {
   const double *s_up, *s_u;
   const PT *s_p;
   const R *s_f;
   int t, slot[3];
-  __device__ __forceinline__ StagedIn(const GridDev &G, const CellIndex &x, const int MODE, unsigned char *raw) {
+  ColR cr;
+  Col64 c64;
+  __device__ __forceinline__ StagedIn(ColR cr_, Col64 c64_) : cr(cr_), c64(c64_) {}
+  __device__ __forceinline__ const ColR &table_r() const { return cr; }
+  __device__ __forceinline__ const Col64 &table64() const { return c64; }
+  // issue the three copy groups (primitives, face fluxes, up and u) of this thread's cell
+  __device__ __forceinline__ void issue(const GridDev &G, const CellIndex &x, const int MODE, unsigned char *raw) {
     t = threadIdx.x;
     double *up = (double *)raw;
     double *u = up + NEQ * CELL_BS_STAGE;
@@ -319,8 +376,9 @@ struct StagedIn {
   __device__ __forceinline__ double u(int v) const { return s_u[v * CELL_BS_STAGE + t]; }
 };
 
-// dirs: the most active directions of any grid of the launch (sizes the dynamic shared
-// memory, cell_stage_bytes<R, PT>(dirs) bytes)
+// Dynamic shared memory: the table slice (slice_bytes<R>()), then for the mixed policy the
+// staged inputs (cell_stage_bytes<R, PT>(dirs); dirs = the most active directions of any
+// grid of the launch).
 template <int MODE, class R, class PT>
 __global__ void __launch_bounds__(CELL_BS_STAGE, cell_min_blocks<PT>())
     k_cell_update(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
@@ -328,22 +386,54 @@ __global__ void __launch_bounds__(CELL_BS_STAGE, cell_min_blocks<PT>())
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   unsigned ia, jb, kc;
-  if (!tile_item<7>(G.tiles[TILE_CELL], (unsigned)bm.first >> 7, threadIdx.x, (unsigned)G.nx, (unsigned)G.ny,
-                    (unsigned)G.nz, ia, jb, kc))
-    return;
-  if (!cell_staged<PT>()) {
-    cell_item<R, PT>(G, ia, jb, kc, MODE);
-    return;
-  }
+  const bool valid = tile_item<7>(G.tiles[TILE_CELL], (unsigned)bm.first >> 7, threadIdx.x, (unsigned)G.nx,
+                                  (unsigned)G.ny, (unsigned)G.nz, ia, jb, kc);
   double dt = 0.0;
   if (MODE != 0) {
     const GridClock ck = *G.clock;
-    if (clock_skip(ck)) return;
+    if (clock_skip(ck)) return;  // the same for the whole block (one grid)
     dt = clock_dt(ck);
   }
+  const unsigned lane = threadIdx.x & 31u;
+  const bool sliced = cell_tile_sliced(G);  // the same for the whole block
+  R *slice = (R *)cell_stage;
+  if (sliced) stage_slice<R>(slice, centre_table<R>(G), G, ia - lane, jb);
   const CellIndex x = cell_index_of(G, ia, jb, kc);
-  const StagedIn<R, PT> in(G, x, MODE, cell_stage);
-  cell_core<R, PT>(G, ia, jb, x, MODE, dt, in);
+  const long long ij = (long long)ia + (long long)G.nx * jb;
+  if (!cell_staged<PT>()) {  // FP64: direct loads of the streamed inputs
+    if (sliced) {
+      cp_async_wait<0>();
+      __syncthreads();
+    }
+    if (!valid) return;
+    if (sliced)
+      cell_core<R, PT>(G, ia, jb, x, MODE, dt,
+                       DirectIn<R, PT, SliceCol<R>, SliceCol<R>>{G, x, SliceCol<R>{slice, lane}, SliceCol<R>{slice, lane}});
+    else
+      cell_core<R, PT>(G, ia, jb, x, MODE, dt,
+                       DirectIn<R, PT>{G, x, global_col(centre_table<R>(G), G, ij), global_col(G.centre, G, ij)});
+    return;
+  }
+  // mixed policy: the FP32 table from the slice, the FP64 metric of con2prim from global
+  unsigned char *inputs = cell_stage + slice_bytes<R>();
+  if (sliced) {
+    StagedIn<R, PT, SliceCol<R>, GlobalCol<double>> in(SliceCol<R>{slice, lane}, global_col(G.centre, G, ij));
+    if (valid) {
+      in.issue(G, x, MODE, inputs);
+      cp_async_wait<3>();  // the slice's group; the three input groups stay in flight
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    if (!valid) return;
+    cell_core<R, PT>(G, ia, jb, x, MODE, dt, in);
+  } else {
+    if (!valid) return;
+    StagedIn<R, PT, GlobalCol<R>, GlobalCol<double>> in(global_col(centre_table<R>(G), G, ij),
+                                                         global_col(G.centre, G, ij));
+    in.issue(G, x, MODE, inputs);
+    cell_core<R, PT>(G, ia, jb, x, MODE, dt, in);
+  }
 }
 
 }  // namespace grhd

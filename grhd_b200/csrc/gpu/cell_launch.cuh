@@ -15,7 +15,7 @@ template <class R, class PT>
 void launch_cell(int mode, const GridDev *grids, const BlockMap *map, int nblocks, int dirs, cudaStream_t s) {
   if (nblocks <= 0) return;
   const unsigned nb = (unsigned)nblocks;
-  const size_t smem = cell_stage_bytes<R, PT>(dirs);
+  const size_t smem = slice_bytes<R>() + cell_stage_bytes<R, PT>(dirs);
   switch (mode) {
     case 0: k_cell_update<0, R, PT><<<nb, CELL_BS, smem, s>>>(grids, map); break;
     case 1: k_cell_update<1, R, PT><<<nb, CELL_BS, smem, s>>>(grids, map); break;
