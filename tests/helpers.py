@@ -20,6 +20,16 @@ def shock_tube(nx=400, rec="weno5", rs="hlle", sensor=False, **kw) -> Problem:
     return Problem.from_keys("sod", **keys)
 
 
+def shock_tube_xy(nx=96, ny=24, rec="mp5", rs="hllc", sensor=False, **kw) -> Problem:
+    """The shock tube on an x-y grid (nz = 1) with a moving left state and 5 % seeded
+    pressure noise, so that every row along y differs: the layout with a y extent and no
+    k extent."""
+    keys = dict(ny=ny, sod_velocity_left=0.3, perturbation="pressure_noise", perturbation_amplitude=0.05,
+                perturbation_time=0.0, perturbation_seed=11)
+    keys.update(kw)
+    return shock_tube(nx=nx, rec=rec, rs=rs, sensor=sensor, **keys)
+
+
 def michel(nx=1024, rec="mp5", rs="hlle", sensor=False, **kw) -> Problem:
     """Michel accretion onto Schwarzschild (M=1), ingoing EF, log r in [1.8, 20], Gamma 4/3,
     sonic radius 8, 1e-3 isentropic density noise at t=0."""

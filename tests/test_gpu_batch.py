@@ -9,7 +9,7 @@ import pytest
 
 from grhd_b200.solver import GpuBatch, GpuGrid
 from oracle.binding import OracleRun
-from tests.helpers import initial_state, michel, rel_l1, shock_tube, torus_2p5d, torus_3d
+from tests.helpers import initial_state, michel, rel_l1, shock_tube, shock_tube_xy, torus_2p5d, torus_3d
 
 pytestmark = pytest.mark.gpu
 
@@ -29,6 +29,7 @@ def _cases():
         (torus_2p5d(nx=64, nz=32), 1e30, 20),
         (torus_3d(nx=24, ny=12, nz=12), 1e30, 6),
         (torus_2p5d(nx=48, nz=24, rec="weno3", rs="hllc", sensor=True), 1e30, 15),
+        (shock_tube_xy(nx=80, ny=20), 1e30, 12),
     ]
 
 

@@ -10,7 +10,7 @@ import pytest
 
 from grhd_b200.solver import GpuGrid
 from oracle.binding import OracleRun
-from tests.helpers import (face_ghost_mask, initial_state, interior, michel, rel_l1, shock_tube,
+from tests.helpers import (face_ghost_mask, initial_state, interior, michel, rel_l1, shock_tube, shock_tube_xy,
                            torus_2p5d, torus_3d)
 
 pytestmark = pytest.mark.gpu
@@ -129,6 +129,16 @@ def test_torus_2p5d_run():
     """Equatorial KS torus, WENO5 + HLLE, 200 x 1 x 100, 40 steps."""
     pb = torus_2p5d(nx=200, nz=100)
     o, g, up, p = run_pair(pb, nsteps=40)
+    assert_parity(pb, o, g, up, p)
+
+
+def test_xy_grid_run():
+    """A grid with a y extent and no k extent (nz = 1): x-y block tiles, y faces without k
+    rows, the cell update reading the metric table from global memory (its shared-memory
+    slice needs a k extent).  Shock tube 96 x 24 with 5 % pressure noise, MP5 + HLLC, 30
+    steps."""
+    pb = shock_tube_xy()
+    o, g, up, p = run_pair(pb, nsteps=30)
     assert_parity(pb, o, g, up, p)
 
 
