@@ -1,6 +1,7 @@
 // cell.cuh -- per-cell device code of the stage update: metric sources, the RK stage
-// combination and con2prim for one cell (cell_item), shared by the stage kernels and the
-// persistent step kernel.
+// combination and con2prim for one cell (cell_core), fed directly from global memory
+// (cell_item: the persistent step kernel, and the stage kernel without a table slice) or
+// through shared-memory staging (k_cell_update).
 #pragma once
 
 #include "common.cuh"

@@ -1,18 +1,21 @@
-// flux.cuh -- face fluxes of one direction as two lean kernels.
+// flux.cuh -- face fluxes of one direction.
 //
-//   k_recon<DIR, REC>   one thread per face: selects the branch of reconstruct_1d_core
-//                       (reconstruction.f90:318-645) from the density and pressure
-//                       stencils, then per variable loads the stencil (boundary fill
-//                       evaluated on load) and writes q_L, q_R with the positivity floors
-//                       (reconstruction.f90:647-655).
-//   k_riemann<DIR, RS>  one thread per face: resolve_riemann_problem (fluxes.f90:56) on
-//                       the reconstructed states, zero flux on degenerate faces
-//                       (evolution.f90:69-71, :122-124).
+//   k_recon<DIR, REC>      one thread per face: selects the branch of reconstruct_1d_core
+//                          (reconstruction.f90:318-645) from the density and pressure
+//                          stencils, then per variable loads the stencil (boundary fill
+//                          evaluated on load) and writes q_L, q_R with the positivity
+//                          floors (reconstruction.f90:647-655).
+//   k_recon_var<DIR, REC>  the same with one thread per (face, variable), for launches
+//                          too small for one thread per face.
+//   k_riemann<DIR, RS>     one thread per face: resolve_riemann_problem (fluxes.f90:56) on
+//                          the reconstructed states, zero flux on degenerate faces
+//                          (evolution.f90:69-71, :122-124).
+//   k_flux<DIR, REC, RS>   both in one kernel, the interface states kept on chip.
 //
-// Splitting the per-face work this way keeps each kernel's code and register footprint
-// small (the reconstruction holds ~75% of the divisions and now runs at high occupancy),
-// and compile-time specialisation on the scheme and the Riemann solver removes the code
-// of the schemes a run does not use.
+// Splitting the per-face work keeps each kernel's code and register footprint small (the
+// reconstruction holds ~75% of the divisions), and compile-time specialisation on the
+// scheme and the Riemann solver removes the code of the schemes a run does not use; the
+// autotuner picks among the split forms and the fused one per launch shape.
 #pragma once
 
 #include "common.cuh"
@@ -154,9 +157,7 @@ __device__ __forceinline__ void recon_one(int br, int lim, const R (&s)[6], R &q
 // 128-thread Riemann blocks), measured on the batched 2.5D torus and the 3D torus: recon
 // 4 (64 registers); Riemann 8 for HLLE (64 registers), HLLC 4 in FP64 (128 registers)
 // and 6 in FP32 (80): HLLC's larger state spills at 64.
-#ifndef GRHD_RECON_MIN_BLOCKS
-#define GRHD_RECON_MIN_BLOCKS 4
-#endif
+constexpr int RECON_MIN_BLOCKS = 4;
 template <int RS, class R>
 constexpr int riemann_min_blocks() { return RS == RS_HLLC ? (sizeof(R) == sizeof(double) ? 4 : 6) : 8; }
 // One thread per face reconstructs all five variables (rolled variable loop): the set-up
@@ -164,7 +165,7 @@ constexpr int riemann_min_blocks() { return RS == RS_HLLC ? (sizeof(R) == sizeof
 // and pressure windows and branch) is paid once per face.  Measured against one thread
 // per (face, variable): FP64 2.5D torus batch +2 %, 3D torus (MP5 + sensor) +24 %.
 template <int DIR, int REC, class R, class PT>
-__global__ void __launch_bounds__(256, GRHD_RECON_MIN_BLOCKS) k_recon(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+__global__ void __launch_bounds__(256, RECON_MIN_BLOCKS) k_recon(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   const Phys P = G.phys;
