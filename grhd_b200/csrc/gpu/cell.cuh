@@ -76,13 +76,14 @@ __device__ __forceinline__ void sources(const Phys &P, const Col &col, const dou
 template <class Col>
 __device__ __forceinline__ CellMetric load_cell_metric(const Col &C) {
   CellMetric m;
-  m.g11 = C(CF_G11); m.g12 = C(CF_G12); m.g13 = C(CF_G13);
-  m.g22 = C(CF_G22); m.g23 = C(CF_G23); m.g33 = C(CF_G33);
-  m.i11 = C(CF_I11); m.i12 = C(CF_I12); m.i13 = C(CF_I13);
-  m.i22 = C(CF_I22); m.i23 = C(CF_I23); m.i33 = C(CF_I33);
-  m.sqg = C(CF_SQG);
+  m.g11_ = C(CF_G11); m.g12_ = C(CF_G12); m.g13_ = C(CF_G13);
+  m.g22_ = C(CF_G22); m.g23_ = C(CF_G23); m.g33_ = C(CF_G33);
+  m.i11_ = C(CF_I11); m.i12_ = C(CF_I12); m.i13_ = C(CF_I13);
+  m.i22_ = C(CF_I22); m.i23_ = C(CF_I23); m.i33_ = C(CF_I33);
+  m.sqg_ = C(CF_SQG);
   return m;
 }
+
 __device__ __forceinline__ CellMetric load_cell_metric(const GridDev &G, long long ij) {
   return load_cell_metric(global_col(G.centre, G, ij));
 }
@@ -139,6 +140,31 @@ struct SliceCol {
   unsigned lane;
   __device__ __forceinline__ T operator()(int fld) const { return s[fld * SLICE_COLS + lane]; }
 };
+// a cell's metric read field by field from a table column where con2prim uses it (for a
+// column in shared memory: no registers held across the root finder)
+template <class Col>
+struct ColMetric {
+  Col c;
+  __device__ __forceinline__ double g11() const { return c(CF_G11); }
+  __device__ __forceinline__ double g12() const { return c(CF_G12); }
+  __device__ __forceinline__ double g13() const { return c(CF_G13); }
+  __device__ __forceinline__ double g22() const { return c(CF_G22); }
+  __device__ __forceinline__ double g23() const { return c(CF_G23); }
+  __device__ __forceinline__ double g33() const { return c(CF_G33); }
+  __device__ __forceinline__ double i11() const { return c(CF_I11); }
+  __device__ __forceinline__ double i12() const { return c(CF_I12); }
+  __device__ __forceinline__ double i13() const { return c(CF_I13); }
+  __device__ __forceinline__ double i22() const { return c(CF_I22); }
+  __device__ __forceinline__ double i23() const { return c(CF_I23); }
+  __device__ __forceinline__ double i33() const { return c(CF_I33); }
+  __device__ __forceinline__ double sqg() const { return c(CF_SQG); }
+};
+// the metric con2prim works with: loaded into registers from global memory, read in place
+// from a shared-memory slice
+template <class T>
+__device__ __forceinline__ CellMetric metric_of(const GlobalCol<T> &c) { return load_cell_metric(c); }
+template <class T>
+__device__ __forceinline__ ColMetric<SliceCol<T>> metric_of(const SliceCol<T> &c) { return ColMetric<SliceCol<T>>{c}; }
 // whether the block's warps share their (i,j) columns (the tile layout above)
 __device__ __forceinline__ bool cell_tile_sliced(const GridDev &G) {
   return G.nz > 1 && G.tiles[TILE_CELL].lx == 5 && G.tiles[TILE_CELL].ly == 0;
@@ -263,13 +289,13 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
     }
     cs[v] = nv;
   }
-  const CellMetric cm = load_cell_metric(in.table64());
+  const auto cm = metric_of(in.table64());
   // mixed policy: seed the root finder with the Lorentz factor of the current primitives
   double W_seed = 0.0;
   if (sizeof(PT) == sizeof(float)) {
     const double a = q[EQ_VX], b = q[EQ_VY], d = q[EQ_VZ];
-    const double vsq = cm.g11 * a * a + cm.g22 * b * b + cm.g33 * d * d +
-                       2.0 * (cm.g12 * a * b + cm.g13 * a * d + cm.g23 * b * d);
+    const double vsq = cm.g11() * a * a + cm.g22() * b * b + cm.g33() * d * d +
+                       2.0 * (cm.g12() * a * b + cm.g13() * a * d + cm.g23() * b * d);
     W_seed = vsq < 1.0 ? 1.0 / sqrt(1.0 - vsq) : 0.0;
   }
   double pr[NEQ];

@@ -506,22 +506,39 @@ __device__ __forceinline__ bool hllc(const Phys &P, const R (&qL)[NEQ], const R 
 // ------------------------------------------------------------------------------------
 // equations.f90:94-424 con2prim (always FP64)
 // ------------------------------------------------------------------------------------
-struct CellMetric {  // symmetric gamma_ij and gamma^ij, sqrt(gamma)
-  double g11, g12, g13, g22, g23, g33;
-  double i11, i12, i13, i22, i23, i33;
-  double sqg;
+// symmetric gamma_ij and gamma^ij, sqrt(gamma) of a cell, held in registers.  con2prim
+// reads a metric through the accessors g11() .. sqg(), so it also takes views that fetch
+// each field where it is used (a cell kernel's shared-memory slice of the table).
+struct CellMetric {
+  double g11_, g12_, g13_, g22_, g23_, g33_;
+  double i11_, i12_, i13_, i22_, i23_, i33_;
+  double sqg_;
+  __device__ __forceinline__ double g11() const { return g11_; }
+  __device__ __forceinline__ double g12() const { return g12_; }
+  __device__ __forceinline__ double g13() const { return g13_; }
+  __device__ __forceinline__ double g22() const { return g22_; }
+  __device__ __forceinline__ double g23() const { return g23_; }
+  __device__ __forceinline__ double g33() const { return g33_; }
+  __device__ __forceinline__ double i11() const { return i11_; }
+  __device__ __forceinline__ double i12() const { return i12_; }
+  __device__ __forceinline__ double i13() const { return i13_; }
+  __device__ __forceinline__ double i22() const { return i22_; }
+  __device__ __forceinline__ double i23() const { return i23_; }
+  __device__ __forceinline__ double i33() const { return i33_; }
+  __device__ __forceinline__ double sqg() const { return sqg_; }
 };
 
 enum C2PFlags : unsigned {
   C2P_FLOOR_PRE = 1u, C2P_CAUSAL = 2u, C2P_BRENT = 4u, C2P_ROOT_FAIL = 8u, C2P_BAD_V = 16u, C2P_SANITISE = 32u
 };
 
-__device__ __forceinline__ double qsq(const CellMetric &m, double S1, double S2, double S3) {
+template <class M>
+__device__ __forceinline__ double qsq(const M &m, double S1, double S2, double S3) {
   // sum over (ii, jj) in the reference's loop order (equations.f90:273-277, :236-242)
   double s = 0.0;
-  s = s + m.i11 * S1 * S1; s = s + m.i12 * S1 * S2; s = s + m.i13 * S1 * S3;
-  s = s + m.i12 * S2 * S1; s = s + m.i22 * S2 * S2; s = s + m.i23 * S2 * S3;
-  s = s + m.i13 * S3 * S1; s = s + m.i23 * S3 * S2; s = s + m.i33 * S3 * S3;
+  s = s + m.i11() * S1 * S1; s = s + m.i12() * S1 * S2; s = s + m.i13() * S1 * S3;
+  s = s + m.i12() * S2 * S1; s = s + m.i22() * S2 * S2; s = s + m.i23() * S2 * S3;
+  s = s + m.i13() * S3 * S1; s = s + m.i23() * S3 * S2; s = s + m.i33() * S3 * S3;
   return s;
 }
 // equations.f90:212-246
@@ -647,19 +664,20 @@ __device__ inline double root_seeded_newton(double g1, double rho_floor, double 
 
 // cons_to_prim, equations.f90:94-205: cons modified in place (intent(inout)); returns flags.
 // W_seed > 0 selects the seeded root finder of the mixed policy; the FP64 path passes 0.
-__device__ inline unsigned cons_to_prim(const Phys &P, const CellMetric &m, double (&cs)[NEQ], double (&pr)[NEQ],
+template <class M>
+__device__ inline unsigned cons_to_prim(const Phys &P, const M &m, double (&cs)[NEQ], double (&pr)[NEQ],
                                         double W_seed = 0.0) {
   unsigned flags = 0;
-  const double lDf = P.rho_floor * m.sqg;
-  const double lTf = P.p_floor * (P.g1 - 1.0) * m.sqg;
+  const double lDf = P.rho_floor * m.sqg();
+  const double lTf = P.p_floor * (P.g1 - 1.0) * m.sqg();
   bool floor_state = false;
   if (cs[EQ_DE] <= lDf) {
     flags |= C2P_FLOOR_PRE;
     floor_state = true;
   } else {
     const double S1 = cs[EQ_VX], S2 = cs[EQ_VY], S3 = cs[EQ_VZ];
-    const double S_sq = S1 * (m.i11 * S1 + m.i12 * S2 + m.i13 * S3) + S2 * (m.i12 * S1 + m.i22 * S2 + m.i23 * S3) +
-                        S3 * (m.i13 * S1 + m.i23 * S2 + m.i33 * S3);
+    const double S_sq = S1 * (m.i11() * S1 + m.i12() * S2 + m.i13() * S3) + S2 * (m.i12() * S1 + m.i22() * S2 + m.i23() * S3) +
+                        S3 * (m.i13() * S1 + m.i23() * S2 + m.i33() * S3);
     const double E = cs[EQ_PR] + cs[EQ_DE];
     const double S_sq_max = rmax(0.0, E * E - cs[EQ_DE] * cs[EQ_DE]) * P.v_max;
     if (S_sq > S_sq_max && S_sq > 1.0e-20) {
@@ -684,16 +702,16 @@ __device__ inline unsigned cons_to_prim(const Phys &P, const CellMetric &m, doub
         floor_state = true;
       } else {
         const double s1 = cs[EQ_VX], s2 = cs[EQ_VY], s3 = cs[EQ_VZ];
-        pr[EQ_DE] = D / (W * m.sqg);
-        pr[EQ_PR] = (V - tau - D) / m.sqg;
-        pr[EQ_VX] = (m.i11 * s1 + m.i12 * s2 + m.i13 * s3) / V;
-        pr[EQ_VY] = (m.i12 * s1 + m.i22 * s2 + m.i23 * s3) / V;
-        pr[EQ_VZ] = (m.i13 * s1 + m.i23 * s2 + m.i33 * s3) / V;
+        pr[EQ_DE] = D / (W * m.sqg());
+        pr[EQ_PR] = (V - tau - D) / m.sqg();
+        pr[EQ_VX] = (m.i11() * s1 + m.i12() * s2 + m.i13() * s3) / V;
+        pr[EQ_VY] = (m.i12() * s1 + m.i22() * s2 + m.i23() * s3) / V;
+        pr[EQ_VZ] = (m.i13() * s1 + m.i23() * s2 + m.i33() * s3) / V;
         const double a = pr[EQ_VX], b = pr[EQ_VY], c = pr[EQ_VZ];
         double vsf = 0.0;
-        vsf = vsf + m.g11 * a * a; vsf = vsf + m.g12 * a * b; vsf = vsf + m.g13 * a * c;
-        vsf = vsf + m.g12 * b * a; vsf = vsf + m.g22 * b * b; vsf = vsf + m.g23 * b * c;
-        vsf = vsf + m.g13 * c * a; vsf = vsf + m.g23 * c * b; vsf = vsf + m.g33 * c * c;
+        vsf = vsf + m.g11() * a * a; vsf = vsf + m.g12() * a * b; vsf = vsf + m.g13() * a * c;
+        vsf = vsf + m.g12() * b * a; vsf = vsf + m.g22() * b * b; vsf = vsf + m.g23() * b * c;
+        vsf = vsf + m.g13() * c * a; vsf = vsf + m.g23() * c * b; vsf = vsf + m.g33() * c * c;
         if (pr[EQ_DE] < P.rho_floor || pr[EQ_PR] < P.p_floor || isnan(pr[EQ_DE]) || isnan(pr[EQ_PR]) ||
             isnan(a) || isnan(b) || isnan(c) || isnan(vsf) || vsf >= P.v_max) {
           flags |= C2P_SANITISE;
@@ -712,7 +730,7 @@ __device__ inline unsigned cons_to_prim(const Phys &P, const CellMetric &m, doub
 // prim_to_cons, equations.f90:30-88 (FP64)
 __device__ __forceinline__ void prim_to_cons(const Phys &P, const CellMetric &m, const double (&q)[NEQ], double (&u)[NEQ]) {
   FaceMetric<double> fm;
-  fm.g11 = m.g11; fm.g12 = m.g12; fm.g13 = m.g13; fm.g22 = m.g22; fm.g23 = m.g23; fm.g33 = m.g33;
+  fm.g11 = m.g11(); fm.g12 = m.g12(); fm.g13 = m.g13(); fm.g22 = m.g22(); fm.g23 = m.g23(); fm.g33 = m.g33();
   double v[3] = {q[EQ_VX], q[EQ_VY], q[EQ_VZ]}, vc[3];
   const double vsq = cap_velocity(fm, v, P.v_max);
   lower(fm, v, vc);
@@ -725,7 +743,7 @@ __device__ __forceinline__ void prim_to_cons(const Phys &P, const CellMetric &m,
   u[EQ_VY] = rhW2 * vc[1];
   u[EQ_VZ] = rhW2 * vc[2];
 #pragma unroll
-  for (int n = 0; n < NEQ; ++n) u[n] = u[n] * m.sqg;
+  for (int n = 0; n < NEQ; ++n) u[n] = u[n] * m.sqg();
 }
 
 }  // namespace grhd
