@@ -444,7 +444,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--batch", type=int, default=32, help="torus grids per GPU stepped as one batch")
-    ap.add_argument("--e2e-streams", type=int, default=4, help="sub-batches (streams) of the end-to-end pipeline")
+    ap.add_argument("--e2e-streams", type=int, default=8, help="sub-batches (streams) of the end-to-end pipeline")
     ap.add_argument("--serve-requests", type=int, default=256, help="serving sample size (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-michel-final-time", type=float, default=2.0)
