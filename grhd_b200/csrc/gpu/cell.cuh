@@ -252,20 +252,20 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) {
     const R a = in.flux(0, 1, v), b = in.flux(0, 0, v);
-    rhs[v] = (double)(-(a - b) / R(dx) + src[v]);
+    rhs[v] = (double)(div_pos(-(a - b), R(dx)) + src[v]);
   }
   if (G.ny > 1) {
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
       const R a = in.flux(1, 1, v), b = in.flux(1, 0, v);
-      rhs[v] = (double)(R(rhs[v]) - (a - b) / R(dy));
+      rhs[v] = (double)(R(rhs[v]) - div_pos(a - b, R(dy)));
     }
   }
   if (G.nz > 1) {
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
       const R a = in.flux(2, 1, v), b = in.flux(2, 0, v);
-      rhs[v] = (double)(R(rhs[v]) - (a - b) / R(dz));
+      rhs[v] = (double)(R(rhs[v]) - div_pos(a - b, R(dz)));
     }
   }
   if (MODE == 0) {

@@ -45,6 +45,17 @@ struct FaceMetric {
 };
 
 template <class R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a || a != a) ? b : a; }
+// n / d for a denominator that is positive (+inf included) or NaN.  The correctly rounded
+// FP64 division runs about three times slower for a zero numerator, and exactly smooth or
+// static regions (a floored atmosphere) produce zero numerators in bulk: a zero never
+// reaches the divider (it divides 1 instead) and is returned as it is -- the quotient, to
+// the bit.  FP32 (the mixed policy's approximate division) divides.
+template <class R> __device__ __forceinline__ R div_pos(R n, R d) {
+  if (sizeof(R) == sizeof(float)) return n / d;
+  const bool z = n == R(0);
+  const R q = (z ? R(1) : n) / d;
+  return (z && d == d) ? n : q;
+}
 template <class R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a || a != a) ? b : a; }
 template <class R> __device__ __forceinline__ R sgn1(R x) { return copysign(R(1), x); }
 template <class R> __device__ __forceinline__ bool fin(R x) { return isfinite(x); }
@@ -118,7 +129,7 @@ template <class R> __device__ __forceinline__ R weno3(R qm, R q0, R qp) {
   R p1 = R(-0.5) * qm + R(1.5) * q0;
   R t0 = q0 - qp, t1 = qm - q0;
   R b0 = t0 * t0, b1 = t1 * t1;
-  R sensor = fabs(b0 - b1) / (rmax(b0, b1) + eps_min);
+  R sensor = div_pos(fabs(b0 - b1), rmax(b0, b1) + eps_min);
   R eh = eps_min + (qm * qm + q0 * q0 + qp * qp) * exp_cw(R(-10) * sensor);
   R e0 = eh + b0, e1 = eh + b1;
   R a0 = d0 / (e0 * e0), a1 = d1 / (e1 * e1);
@@ -161,7 +172,7 @@ template <class R> __device__ __forceinline__ R weno5(R q_2, R q_1, R q0, R q1, 
 // reconstruction.f90:222-254, q(-2:2)
 template <class R> __device__ __forceinline__ R mp5(R q_2, R q_1, R q0, R q1, R q2) {
   const R alpha = R(4), eps = R(1.0e-10);
-  R val_L = (R(2) * q_2 - R(13) * q_1 + R(47) * q0 + R(27) * q1 - R(3) * q2) / R(60);
+  R val_L = div_pos(R(2) * q_2 - R(13) * q_1 + R(47) * q0 + R(27) * q1 - R(3) * q2, R(60));
   R val_mp = q0 + minmod_2(q1 - q0, alpha * (q0 - q_1));
   if ((val_L - q0) * (val_L - val_mp) < eps) return val_L;
   R d_jm1 = q_2 - R(2) * q_1 + q0;
@@ -172,7 +183,7 @@ template <class R> __device__ __forceinline__ R mp5(R q_2, R q_1, R q0, R q1, R 
   R val_ul = q0 + alpha * (q0 - q_1);
   R val_av = R(0.5) * (q0 + q1);
   R val_md = val_av - R(0.5) * dm4_jph;
-  R val_lc = q0 + R(0.5) * (q0 - q_1) + R(4) * dm4_jmh / R(3);
+  R val_lc = q0 + R(0.5) * (q0 - q_1) + div_pos(R(4) * dm4_jmh, R(3));
   R vmin = rmax(rmin(rmin(q0, q1), val_md), rmin(rmin(q0, val_ul), val_lc));
   R vmax = rmin(rmax(rmax(q0, q1), val_md), rmax(rmax(q0, val_ul), val_lc));
   return val_L + minmod_2(vmin - val_L, vmax - val_L);
@@ -295,7 +306,8 @@ __device__ __forceinline__ void hlle(const Phys &P, const R (&qL)[NEQ], const R 
     for (int n = 0; n < NEQ; ++n) flux[n] = R(0);
   } else {
 #pragma unroll
-    for (int n = 0; n < NEQ; ++n) flux[n] = (ap * fL[n] - am * fR[n] + ap * am * (uR[n] - uL[n])) / (ap - am);
+    for (int n = 0; n < NEQ; ++n)  // ap - am > 0 here (or NaN)
+      flux[n] = div_pos(ap * fL[n] - am * fR[n] + ap * am * (uR[n] - uL[n]), ap - am);
   }
 }
 
@@ -714,9 +726,9 @@ __device__ inline unsigned cons_to_prim(const Phys &P, const M &m, double (&cs)[
         const double s1 = cs[EQ_VX], s2 = cs[EQ_VY], s3 = cs[EQ_VZ];
         pr[EQ_DE] = D / (W * m.sqg());
         pr[EQ_PR] = (V - tau - D) / m.sqg();
-        pr[EQ_VX] = (m.i11() * s1 + m.i12() * s2 + m.i13() * s3) / V;
-        pr[EQ_VY] = (m.i12() * s1 + m.i22() * s2 + m.i23() * s3) / V;
-        pr[EQ_VZ] = (m.i13() * s1 + m.i23() * s2 + m.i33() * s3) / V;
+        pr[EQ_VX] = div_pos(m.i11() * s1 + m.i12() * s2 + m.i13() * s3, V);  // V > 0 here
+        pr[EQ_VY] = div_pos(m.i12() * s1 + m.i22() * s2 + m.i23() * s3, V);
+        pr[EQ_VZ] = div_pos(m.i13() * s1 + m.i23() * s2 + m.i33() * s3, V);
         const double a = pr[EQ_VX], b = pr[EQ_VY], c = pr[EQ_VZ];
         double vsf = 0.0;
         vsf = vsf + m.g11() * a * a; vsf = vsf + m.g12() * a * b; vsf = vsf + m.g13() * a * c;
