@@ -163,7 +163,13 @@ template <class R> __device__ __forceinline__ R weno5(R q_2, R q_1, R q0, R q1, 
     a2 = d2 * (R(1) + (tau5 / (eps + b2)));
   }
   R s = a0 + a1 + a2;
-  R w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+  R w0, w1, w2;
+  if (sizeof(R) == sizeof(float)) {  // mixed policy: one reciprocal for the three weights
+    const R inv_s = R(1) / s;
+    w0 = a0 * inv_s; w1 = a1 * inv_s; w2 = a2 * inv_s;
+  } else {
+    w0 = a0 / s; w1 = a1 / s; w2 = a2 / s;
+  }
   R p0 = R(1.0 / 3.0) * q0 + R(5.0 / 6.0) * q1 - R(1.0 / 6.0) * q2;
   R p1 = -(R(1.0 / 6.0) * q_1) + R(5.0 / 6.0) * q0 + R(1.0 / 3.0) * q1;
   R p2 = R(1.0 / 3.0) * q_2 - R(7.0 / 6.0) * q_1 + R(11.0 / 6.0) * q0;
@@ -304,6 +310,10 @@ __device__ __forceinline__ void hlle(const Phys &P, const R (&qL)[NEQ], const R 
   if (fabs(ap - am) < R(1.0e-14)) {
 #pragma unroll
     for (int n = 0; n < NEQ; ++n) flux[n] = R(0);
+  } else if (sizeof(R) == sizeof(float)) {  // mixed policy: one reciprocal for the five components
+    const R inv = R(1) / (ap - am);
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) flux[n] = (ap * fL[n] - am * fR[n] + ap * am * (uR[n] - uL[n])) * inv;
   } else {
 #pragma unroll
     for (int n = 0; n < NEQ; ++n)  // ap - am > 0 here (or NaN)
