@@ -149,26 +149,27 @@ template <class R> __device__ __forceinline__ R weno5(R q_2, R q_1, R q0, R q1, 
   a = q_2 - R(2) * q_1 + q0; b = q_2 - R(4) * q_1 + R(3) * q0;
   R b2 = c1312 * (a * a) + R(0.25) * (b * b);
   R tau5 = fabs(b0 - b2);
-  R a0, a1, a2;
+  R w0, w1, w2;
   if (sizeof(R) == sizeof(double) && tau5 == R(0) && b1 == b1) {
     // an exactly smooth stencil (a uniform atmosphere, say): every tau5 / (eps + b_k) is +0
-    // (tau5 == 0 means b0 and b2 are not NaN; each eps + b_k >= eps > 0 or +inf), and the
-    // correctly rounded FP64 division takes a long path for a zero numerator
-    a0 = d0 * (R(1) + R(0));
-    a1 = d1 * (R(1) + R(0));
-    a2 = d2 * (R(1) + R(0));
-  } else {
-    a0 = d0 * (R(1) + (tau5 / (eps + b0)));
-    a1 = d1 * (R(1) + (tau5 / (eps + b1)));
-    a2 = d2 * (R(1) + (tau5 / (eps + b2)));
-  }
-  R s = a0 + a1 + a2;
-  R w0, w1, w2;
-  if (sizeof(R) == sizeof(float)) {  // mixed policy: one reciprocal for the three weights
-    const R inv_s = R(1) / s;
-    w0 = a0 * inv_s; w1 = a1 * inv_s; w2 = a2 * inv_s;
-  } else {
+    // (tau5 == 0 means b0 and b2 are not NaN; each eps + b_k >= eps > 0 or +inf), so the
+    // alphas are d_k and the weights the constants d_k / (d0 + d1 + d2), folded at compile
+    // time with the same correctly rounded arithmetic.  The FP64 divisions skipped here run
+    // about three times slower than usual for zero numerators.
+    const R a0 = d0 * (R(1) + R(0)), a1 = d1 * (R(1) + R(0)), a2 = d2 * (R(1) + R(0));
+    const R s = a0 + a1 + a2;
     w0 = a0 / s; w1 = a1 / s; w2 = a2 / s;
+  } else {
+    const R a0 = d0 * (R(1) + (tau5 / (eps + b0)));
+    const R a1 = d1 * (R(1) + (tau5 / (eps + b1)));
+    const R a2 = d2 * (R(1) + (tau5 / (eps + b2)));
+    const R s = a0 + a1 + a2;
+    if (sizeof(R) == sizeof(float)) {  // mixed policy: one reciprocal for the three weights
+      const R inv_s = R(1) / s;
+      w0 = a0 * inv_s; w1 = a1 * inv_s; w2 = a2 * inv_s;
+    } else {
+      w0 = a0 / s; w1 = a1 / s; w2 = a2 / s;
+    }
   }
   R p0 = R(1.0 / 3.0) * q0 + R(5.0 / 6.0) * q1 - R(1.0 / 6.0) * q2;
   R p1 = -(R(1.0 / 6.0) * q_1) + R(5.0 / 6.0) * q0 + R(1.0 / 3.0) * q1;
