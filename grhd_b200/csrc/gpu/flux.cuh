@@ -74,16 +74,27 @@ __device__ __forceinline__ double load_var(const PT *__restrict__ P, const GridD
   return out;
 }
 
-// Stencil window m = lo..hi (cells face-2+m along DIR; 0 elsewhere) of variable v for a
-// face whose window leaves the grid: boundary fill on load.  The fused face kernel calls
-// it out of line, so its interior path keeps the registers for the reconstruction and
-// the Riemann solver (measured: mixed 2.5D torus batch +7 %, 3D torus +16 %).  k_recon
-// keeps the boundary fill inline: the call costs its FP64 interior path 7 %.
+// All five variables of the window cells m = lo..hi (0 elsewhere) of a face whose window
+// leaves the grid, each cell's boundary fill evaluated once: w[v][m].  Out of line, with w
+// in the caller's local memory, so the interior path keeps its registers and a warp that
+// holds a few such faces among interior ones (two warps of each 401-face row along x)
+// pays one short detour per face instead of one per (variable, cell).  Measured against
+// boundary fill per (variable, cell): fused FP32 face kernel along x -27 % (mixed 2.5D
+// torus batch +12 %, 3D torus +24 %); FP64 reconstruction along x -9 % (2.5D) and -37 %
+// (3D torus, MP5 with the sensor).
 template <int DIR, class R, class PT>
-__device__ __noinline__ void edge_stencil(const PT *__restrict__ P, const GridDev &G, const FaceIndex &x, int v, int lo,
-                                          int hi, R (&s)[6]) {
+__device__ __noinline__ void edge_window(const PT *__restrict__ P, const GridDev &G, const FaceIndex &x, int lo, int hi,
+                                         R (&w)[NEQ][6]) {
+#pragma unroll 1
+  for (int m = 0; m < 6; ++m) {
+    double q[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (m >= lo && m <= hi) {
+      const int c = x.face - 2 + m;
+      load_cell<DIR>(P, G, DIR == 1 ? c : x.i, DIR == 2 ? c : x.j, DIR == 3 ? c : x.k, q);
+    }
 #pragma unroll
-  for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? R(load_var<DIR>(P, G, x, x.face - 2 + m, v)) : R(0);
+    for (int v = 0; v < NEQ; ++v) w[v][m] = (m >= lo && m <= hi) ? R(q[v]) : R(0);
+  }
 }
 
 // branch selection of reconstruct_1d_core from the density and pressure stencils
@@ -189,9 +200,10 @@ __global__ void __launch_bounds__(256, RECON_MIN_BLOCKS) k_recon(const GridDev *
     const int c0 = x.face - 2 + lo;
     base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
   }
+  R ew[NEQ][6];  // an edge face's window, boundary-filled (local memory)
+  if (!inside) edge_window<DIR>(Pin, G, x, lo, hi, ew);
   auto ld = [&](int w, int m) -> R {
-    return inside ? R((double)GRHD_LDP(&Pin[w * G.pplane + base + m * stride]))
-                  : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, w));
+    return inside ? R((double)GRHD_LDP(&Pin[w * G.pplane + base + m * stride])) : ew[w][m];
   };
   int br = BR_GODUNOV;
   if (REC != REC_GODUNOV) {
@@ -219,7 +231,7 @@ __global__ void __launch_bounds__(256, RECON_MIN_BLOCKS) k_recon(const GridDev *
       for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? R((double)GRHD_LDP(row + m * ustride)) : R(0);
     } else {
 #pragma unroll
-      for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? R(load_var<DIR>(Pin, G, x, x.face - 2 + m, v)) : R(0);
+      for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ew[v][m] : R(0);
     }
     R qL, qR;
     recon_one<REC>(br, lim, s, qL, qR);
@@ -339,16 +351,19 @@ __device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned
     base = (long long)cell_index(G, DIR == 1 ? c0 : x.i, DIR == 2 ? c0 : x.j, DIR == 3 ? c0 : x.k) - lo * stride;
   }
   // window m = a..b of variable w; the interior case reads P at 32-bit offsets from the
-  // variable's row pointer
+  // variable's row pointer, an edge face its window of boundary-filled cells
   const long long pplane = G.pplane;
   const unsigned ustride = (unsigned)stride;
+  R ew[NEQ][6];
+  if (!inside) edge_window<DIR>(Pin, G, x, lo, hi, ew);
   auto window = [&](int w, int a, int b, R(&out)[6]) {
     if (inside) {
       const PT *row = Pin + (base + (long long)w * pplane);
 #pragma unroll
       for (int m = 0; m < 6; ++m) out[m] = (m >= a && m <= b) ? R((double)GRHD_LDP(row + m * ustride)) : R(0);
     } else {
-      edge_stencil<DIR>(Pin, G, x, w, a, b, out);
+#pragma unroll
+      for (int m = 0; m < 6; ++m) out[m] = (m >= a && m <= b) ? ew[w][m] : R(0);
     }
   };
   int br = BR_GODUNOV;
