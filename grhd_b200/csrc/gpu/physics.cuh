@@ -584,6 +584,39 @@ __device__ __forceinline__ void residual(double g1, double W, double D, double t
   res = (V * V) * (1.0 - 1.0 / (W * W)) - Q2;
   dres = 2.0 * V * (dV * (W3 - W) + V) / W3;
 }
+// Mixed policy only: reciprocal of a positive normal x in FP64, by Newton-Raphson
+// refinement (r <- r + r (1 - x r), each step doubling the correct bits) of the hardware
+// approximation rcp.approx.ftz.f64.  Two steps: on 2.7e8 random x with exponents in
+// [-60, 60] the result equals the correctly rounded 1.0 / x bit for bit (one step: 1e-12
+// relative).  Zero, subnormal or infinite x give NaN or 0; callers pass positive normals.
+__device__ __forceinline__ double rcp_mixed(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+// The residual of equations.f90:212-246 for the mixed policy's root finder: the same
+// expressions with one reciprocal of den and one of W shared by its four quotients.
+__device__ __forceinline__ void residual_mixed(double g1, double W, double D, double tau, double Q2,
+                                               double &res, double &dres) {
+  const double W2 = W * W;
+  const double den = g1 * W2 - 1.0;  // > 0: g1 > 1, W >= 1
+  const double iden = rcp_mixed(den);
+  const double V = (g1 * W2 * (tau + D) - D * W) * iden;
+  const double dV = (g1 * W * (D * W - 2.0 * (tau + D)) + D) * (iden * iden);
+  const double iW = rcp_mixed(W);
+  const double iW2 = iW * iW;
+  res = (V * V) * (1.0 - iW2) - Q2;
+  dres = 2.0 * V * (dV * (W2 * W - W) + V) * (iW2 * iW);
+}
+// the reference's starting point for Newton (the bracket midpoint): no seed
+struct NoSeed {
+  static constexpr bool seeded = false;
+  __device__ __forceinline__ double operator()() const { return 0.0; }
+};
+
 // equations.f90:343-424 (per-call locals reproduce the reference: its SAVE'd d, e are
 // written in the first iteration before being read)
 __device__ inline double root_brent(double g1, double rho_floor, double D, double tau, double Q2) {
@@ -657,25 +690,28 @@ __device__ inline double root_safe_newton(double g1, double rho_floor, double D,
   return root_brent(g1, rho_floor, D, tau, Q2);
 }
 
-// Mixed-policy root finder: the same residual and bracket [1, max(1e3, 2 W_guess)] as
-// root_safe_newton, but Newton starts from W_seed (the Lorentz factor of the cell's
-// current primitives, a few 1e-3 off the root after one stage) instead of the bracket
+// Mixed-policy root finder: the residual and bracket [1, max(1e3, 2 W_guess)] of
+// root_safe_newton (the residual with shared reciprocals), but Newton starts from the seed
+// (the Lorentz factor of the cell's current primitives, a few 1e-3 off the root after one
+// stage, evaluated only for a cell that reaches the root finder) instead of the bracket
 // midpoint, so it converges in a few iterations instead of ~10 bisections plus Newton.
 // f(1) = -Q2 <= 0 analytically (V is finite at W = 1 since g1 > 1), so the lower end needs
 // no evaluation.  Not converged after 20 iterations, or no sign change at the upper end:
 // the reference iteration decides (same result class as the FP64 path).
+template <class Seed>
 __device__ inline double root_seeded_newton(double g1, double rho_floor, double D, double tau, double Q2,
-                                            double W_seed, unsigned &flags) {
+                                            const Seed &seed, unsigned &flags) {
   const double x_acc = 1.0e-10;
   if (Q2 < 1.0e-14) return 1.0;  // root_safe_newton: |f(1)| = Q2 < 1e-14 returns W = 1
-  const double Wg = (sqrt(Q2) + D) / rmax(D, rho_floor);
+  const double W_seed = seed();
+  const double Wg = (sqrt(Q2) + D) * rcp_mixed(rmax(D, rho_floor));
   const double x2 = rmax(1.0e3, Wg * 2.0);
   double lo = 1.0, hi = x2;
   double root = (W_seed > 1.0 && W_seed < x2) ? W_seed : 0.5 * (1.0 + x2);
   double f, df;
   bool hi_checked = false;
   for (int it = 0; it < 20; ++it) {
-    residual(g1, root, D, tau, Q2, f, df);
+    residual_mixed(g1, root, D, tau, Q2, f, df);
     if (!(f == f) || !(df == df)) break;
     if (f < 0.0) lo = root; else { hi = root; hi_checked = true; }
     double next = root - f / df;
@@ -683,7 +719,7 @@ __device__ inline double root_seeded_newton(double g1, double rho_floor, double 
     if (!(next > lo && next < hi)) {             // outside the bracket: bisect
       if (!hi_checked) {                         // confirm the upper end brackets the root first
         double fh, dfh;
-        residual(g1, x2, D, tau, Q2, fh, dfh);
+        residual_mixed(g1, x2, D, tau, Q2, fh, dfh);
         if (!(fh > 0.0)) break;
         hi_checked = true;
       }
@@ -696,10 +732,11 @@ __device__ inline double root_seeded_newton(double g1, double rho_floor, double 
 }
 
 // cons_to_prim, equations.f90:94-205: cons modified in place (intent(inout)); returns flags.
-// W_seed > 0 selects the seeded root finder of the mixed policy; the FP64 path passes 0.
-template <class M>
+// A seed (Seed::seeded) selects the mixed policy's root finder and its primitive recovery
+// with shared reciprocals; the FP64 path passes NoSeed and follows the reference exactly.
+template <class M, class Seed = NoSeed>
 __device__ inline unsigned cons_to_prim(const Phys &P, const M &m, double (&cs)[NEQ], double (&pr)[NEQ],
-                                        double W_seed = 0.0) {
+                                        const Seed &seed = Seed()) {
   unsigned flags = 0;
   const double lDf = P.rho_floor * m.sqg();
   const double lTf = P.p_floor * (P.g1 - 1.0) * m.sqg();
@@ -722,24 +759,35 @@ __device__ inline unsigned cons_to_prim(const Phys &P, const M &m, double (&cs)[
     }
     const double D = cs[EQ_DE], tau = cs[EQ_PR];
     const double Q2 = qsq(m, cs[EQ_VX], cs[EQ_VY], cs[EQ_VZ]);
-    const double W = W_seed > 0.0 ? root_seeded_newton(P.g1, P.rho_floor, D, tau, Q2, W_seed, flags)
-                                  : root_safe_newton(P.g1, P.rho_floor, D, tau, Q2, flags);
+    double W;
+    if (Seed::seeded) W = root_seeded_newton(P.g1, P.rho_floor, D, tau, Q2, seed, flags);
+    else W = root_safe_newton(P.g1, P.rho_floor, D, tau, Q2, flags);
     if (W < 1.0) {
       flags |= C2P_ROOT_FAIL;
       floor_state = true;
     } else {
       const double den = P.g1 * (W * W) - 1.0;
-      const double V = (P.g1 * (W * W) * (tau + D) - D * W) / den;
+      const double V = Seed::seeded ? (P.g1 * (W * W) * (tau + D) - D * W) * rcp_mixed(den)
+                                    : (P.g1 * (W * W) * (tau + D) - D * W) / den;
       if (V <= 0.0 || isnan(V)) {
         flags |= C2P_BAD_V;
         floor_state = true;
       } else {
         const double s1 = cs[EQ_VX], s2 = cs[EQ_VY], s3 = cs[EQ_VZ];
-        pr[EQ_DE] = D / (W * m.sqg());
-        pr[EQ_PR] = (V - tau - D) / m.sqg();
-        pr[EQ_VX] = div_pos(m.i11() * s1 + m.i12() * s2 + m.i13() * s3, V);  // V > 0 here
-        pr[EQ_VY] = div_pos(m.i12() * s1 + m.i22() * s2 + m.i23() * s3, V);
-        pr[EQ_VZ] = div_pos(m.i13() * s1 + m.i23() * s2 + m.i33() * s3, V);
+        if (Seed::seeded) {  // mixed policy: one reciprocal of V and one of sqrt(gamma)
+          const double isq = rcp_mixed(m.sqg()), iV = rcp_mixed(V);
+          pr[EQ_DE] = D * rcp_mixed(W) * isq;
+          pr[EQ_PR] = (V - tau - D) * isq;
+          pr[EQ_VX] = (m.i11() * s1 + m.i12() * s2 + m.i13() * s3) * iV;
+          pr[EQ_VY] = (m.i12() * s1 + m.i22() * s2 + m.i23() * s3) * iV;
+          pr[EQ_VZ] = (m.i13() * s1 + m.i23() * s2 + m.i33() * s3) * iV;
+        } else {
+          pr[EQ_DE] = D / (W * m.sqg());
+          pr[EQ_PR] = (V - tau - D) / m.sqg();
+          pr[EQ_VX] = div_pos(m.i11() * s1 + m.i12() * s2 + m.i13() * s3, V);  // V > 0 here
+          pr[EQ_VY] = div_pos(m.i12() * s1 + m.i22() * s2 + m.i23() * s3, V);
+          pr[EQ_VZ] = div_pos(m.i13() * s1 + m.i23() * s2 + m.i33() * s3, V);
+        }
         const double a = pr[EQ_VX], b = pr[EQ_VY], c = pr[EQ_VZ];
         double vsf = 0.0;
         vsf = vsf + m.g11() * a * a; vsf = vsf + m.g12() * a * b; vsf = vsf + m.g13() * a * c;
