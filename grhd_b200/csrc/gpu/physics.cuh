@@ -656,12 +656,15 @@ __device__ inline double root_brent(double g1, double rho_floor, double D, doubl
 // equations.f90:249-340
 __device__ inline double root_safe_newton(double g1, double rho_floor, double D, double tau, double Q2, unsigned &flags) {
   const double x_acc = 1.0e-10, x1 = 1.0;
+  double f_low, f_high, df, f, root, dx, dx_old, tmp;
+  residual(g1, x1, D, tau, Q2, f_low, df);
+  // The reference evaluates the upper end before this test; nothing of it reaches the
+  // return, so a cell at rest in the atmosphere (f(1) = -Q2 ~ 0) skips it.
+  if (fabs(f_low) < 1.0e-14) return x1;
   const double Wg = (sqrt(Q2) + D) / rmax(D, rho_floor);
   const double x2 = rmax(1.0e3, Wg * 2.0);
-  double x_low = x1, x_high = x2, f_low, f_high, df, f, root, dx, dx_old, tmp;
-  residual(g1, x1, D, tau, Q2, f_low, df);
+  double x_low = x1, x_high = x2;
   residual(g1, x2, D, tau, Q2, f_high, df);
-  if (fabs(f_low) < 1.0e-14) return x_low;
   if (fabs(f_high) < 1.0e-14) return x_high;
   if (sgn1(f_low) * sgn1(f_high) > 0.0) return -1.0;
   if (f_low < 0.0) { x_low = x1; x_high = x2; } else { x_high = x1; x_low = x2; }
