@@ -426,13 +426,14 @@ __device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned
 }
 
 
-// Resident 128-thread blocks per SM for the fused kernel: the FP32 instantiation (mixed
-// policy) is latency-bound and runs fastest at 10 (48 registers; measured on the batched
-// 2.5D torus and the 3D torus); the FP64 one keeps its registers.
-template <class R>
-constexpr int flux_min_blocks() { return sizeof(R) == sizeof(float) ? 10 : 1; }
+// Resident 128-thread blocks per SM for the fused kernel.  FP32 (mixed policy): 10 with
+// HLLE (48 registers; 8 and 12 measured 2.5 % and 0-1 % slower on the batched 2.5D torus),
+// 8 with HLLC, whose larger state spills at 48 (64 registers; 3D torus +2.8 %, its x faces
+// -8 %).  The FP64 instantiation keeps its registers.
+template <int RS, class R>
+constexpr int flux_min_blocks() { return sizeof(R) == sizeof(float) ? (RS == RS_HLLC ? 8 : 10) : 1; }
 template <int DIR, int REC, int RS, class R, class PT>
-__global__ void __launch_bounds__(FLUX_BS, flux_min_blocks<R>())
+__global__ void __launch_bounds__(FLUX_BS, flux_min_blocks<RS, R>())
     k_flux(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
   __shared__ R sq[2 * NEQ][FLUX_BS];
   const BlockMap bm = map[blockIdx.x];
