@@ -277,9 +277,10 @@ def run_ours(args):
     close_batch(g64, b64)
 
     # End to end through the C-ABI with page-locked host buffers: every step uploads each
-    # grid's conserved state, recovers the primitives, steps, and downloads the conserved
-    # state.  The grids are split into sub-batches on their own streams and every call is
-    # asynchronous, so one sub-batch's copies overlap another's kernels.
+    # grid's conserved state, recovers the primitives (one launch per sub-batch), steps,
+    # and downloads the conserved state.  The grids are split into sub-batches on their own
+    # streams and every call is asynchronous, so one sub-batch's copies overlap another's
+    # kernels.
     from grhd_b200 import native as N
     nsub = max(1, min(args.e2e_streams, nb))
     subs = []
@@ -303,7 +304,7 @@ def run_ours(args):
             ptrs = work[k:k + len(grids)]
             for g, pu in zip(grids, ptrs):
                 assert lib.grhd2_gpu_upload_async(g._h, pu, None) == 0
-                assert lib.grhd2_gpu_cons_to_prim_all(g._h) == 0
+            assert lib.grhd2_gpu_batch_cons_to_prim(bq._b) == 0
             bq.step(1, graph=True)
             for g, pu in zip(grids, ptrs):
                 assert lib.grhd2_gpu_download_async(g._h, pu, None) == 0
@@ -354,9 +355,10 @@ def run_ours(args):
         "clocks": clocks,
         "e2e": {"value": world * nb * ncell * args.steps / (ms_e * 1e-3), "unit": "zone-updates/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
-                "path": f"the {nb} grids in {nsub} sub-batches on their own streams; per step and grid "
-                        "grhd2_gpu_upload_async(up) + grhd2_gpu_cons_to_prim_all, grhd2_gpu_batch_step per "
-                        "sub-batch, grhd2_gpu_download_async(up); page-locked host buffers"},
+                "path": f"the {nb} grids in {nsub} sub-batches on their own streams; per step "
+                        "grhd2_gpu_upload_async(up) per grid, grhd2_gpu_batch_cons_to_prim and "
+                        "grhd2_gpu_batch_step per sub-batch, grhd2_gpu_download_async(up) per grid; "
+                        "page-locked host buffers"},
         "gpu_launches": sum(launches.values()) * args.steps,
         "kernels_ms_per_step": per_step,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1610,6 +1610,26 @@ int grhd2_gpu_batch_step(grhd2_gpu_batch *b, int nsteps, int use_graph) {
   return batch_steps(b, nsteps, use_graph != 0);
 }
 
+int grhd2_gpu_batch_cons_to_prim(grhd2_gpu_batch *b) {
+  if (!b) return GRHD2_ERR_ARG;
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  for (size_t k = 0; k < b->m.size(); ++k) {
+    grhd2_gpu *h = b->m[k];
+    if (int rc = ready(h, false)) return bfail(b, rc, "grid %d: %s", (int)k, h->err.c_str());
+    if (!h->cons_set) return bfail(b, GRHD2_ERR_STATE, "grid %d: conserved state not uploaded", (int)k);
+  }
+  if (int rc = refresh_batch(b)) return rc;
+  for (const auto &grp : b->groups) {
+    if (grp.nb[K_CELL] <= 0) continue;
+    const unsigned nb = (unsigned)grp.nb[K_CELL];
+    if (grp.mixed) k_c2p_batch<float><<<nb, CELL_BS, 0, b->stream>>>(b->d_grids, grp.d_map + grp.off[K_CELL]);
+    else k_c2p_batch<double><<<nb, CELL_BS, 0, b->stream>>>(b->d_grids, grp.d_map + grp.off[K_CELL]);
+    if (int rc = blaunch_check(b, "c2p_batch")) return rc;
+  }
+  for (grhd2_gpu *h : b->m) h->prims_set = true;
+  return GRHD2_OK;
+}
+
 int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *steps, int *active) {
   if (!b || k < 0 || k >= (int)b->m.size()) return bfail(b, GRHD2_ERR_ARG, "grid index out of range");
   grhd2_gpu *h = b->m[k];

@@ -51,6 +51,33 @@ __global__ void k_c2p_all(const GridDev G, const Phys P, PT *__restrict__ Pout, 
   c2p_count(cnt, fl);
 }
 
+// The same con2prim over every cell of a batch's scheme group in one launch (the block map
+// of the cell update's tiles).  A 400x1x200 torus alone is one wave of ~18 us, bound by
+// the latency of its torus cells' ~30 residual evaluations; launched together, the grids'
+// waves overlap instead of running one after another.
+template <class PT>
+__global__ void __launch_bounds__(CELL_BS_STAGE, 8)
+    k_c2p_batch(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
+  const BlockMap bm = map[blockIdx.x];
+  const GridDev &G = grids[bm.grid];
+  unsigned ia, jb, kc;
+  if (!tile_item<7>(G.tiles[TILE_CELL], (unsigned)bm.first >> 7, threadIdx.x, (unsigned)G.nx, (unsigned)G.ny,
+                    (unsigned)G.nz, ia, jb, kc))
+    return;
+  const CellIndex x = cell_index_of(G, ia, jb, kc);
+  const long long ij = (long long)ia + (long long)G.nx * jb;
+  double *__restrict__ UP = G.UP;
+  PT *__restrict__ Pout = (PT *)G.P;
+  const long long pl = G.pplane;
+  double cs[NEQ], pr[NEQ];
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) cs[v] = UP[v * pl + x.c];
+  const unsigned fl = cons_to_prim(G.phys, load_cell_metric(G, ij), cs, pr);
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) { UP[v * pl + x.c] = cs[v]; Pout[v * pl + x.c] = (PT)pr[v]; }
+  c2p_count(G.cnt, fl);
+}
+
 template <class PT>
 __global__ void k_p2c_all(const GridDev G, const Phys P, const PT *__restrict__ Pin, double *__restrict__ UP) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;

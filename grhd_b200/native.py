@@ -124,6 +124,7 @@ GPU_SYMBOLS = {
     "grhd2_gpu_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(_VP)]),
     "grhd2_gpu_batch_set_clock": (C.c_int, [_VP, C.c_int, C.c_double, C.c_double, C.c_int64]),
     "grhd2_gpu_batch_step": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "grhd2_gpu_batch_cons_to_prim": (C.c_int, [_VP]),
     "grhd2_gpu_batch_get_clock": (C.c_int, [_VP, C.c_int, c_double_p, C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int)]),
     "grhd2_gpu_batch_profile_step": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_char_p),

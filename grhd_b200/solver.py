@@ -303,6 +303,11 @@ class GpuBatch:
         """Enqueue nsteps batched steps (asynchronous)."""
         self._check(self.lib.grhd2_gpu_batch_step(self._b, nsteps, 1 if graph else 0))
 
+    def cons_to_prim(self):
+        """cons_to_prim of every grid's uploaded conserved state, one launch per scheme
+        group (asynchronous; the results of GpuGrid.cons_to_prim on each grid)."""
+        self._check(self.lib.grhd2_gpu_batch_cons_to_prim(self._b))
+
     def clocks(self):
         """(t, steps, active) arrays of every grid in one device read (synchronises)."""
         n = len(self.grids)

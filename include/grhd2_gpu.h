@@ -248,6 +248,11 @@ int grhd2_gpu_batch_set_clock(grhd2_gpu_batch *b, int k, double t0, double final
 /* Advance every grid that has not reached its final time by up to nsteps steps (one CUDA
  * graph per step when use_graph != 0).  Asynchronous; grids that finish early stop. */
 int grhd2_gpu_batch_step(grhd2_gpu_batch *b, int nsteps, int use_graph);
+/* grhd2_gpu_cons_to_prim_all of every grid of the batch in one launch per scheme group
+ * (same results and counters).  Asynchronous on the batch's stream: for a caller that
+ * uploads the conserved state of many grids (grhd2_gpu_upload_async) and recovers their
+ * primitives before stepping. */
+int grhd2_gpu_batch_cons_to_prim(grhd2_gpu_batch *b);
 /* Read grid k's clock (synchronises the stream). */
 int grhd2_gpu_batch_get_clock(grhd2_gpu_batch *b, int k, double *t, int64_t *steps, int *active);
 /* Per-launch timing of one batched step (names/ms as in grhd2_gpu_profile_step). */

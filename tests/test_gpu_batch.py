@@ -140,6 +140,41 @@ def test_batch_equals_alone_with_mixed_member():
         g.close()
 
 
+def test_batch_cons_to_prim_equals_per_grid():
+    """grhd2_gpu_batch_cons_to_prim: every grid's primitives, conserved state and counters
+    equal grhd2_gpu_cons_to_prim_all's on the same uploaded state (FP64 grids of six
+    schemes and layouts, and a mixed-precision grid, after a few steps)."""
+    s = _stream()
+    pbs = [pb for pb, _, _ in _cases()] + [torus_2p5d(nx=48, nz=24)]
+    precs = ["fp64"] * (len(pbs) - 1) + ["mixed"]
+    grids = [_make(pb, s, pr)[0] for pb, pr in zip(pbs, precs)]
+    b = GpuBatch(grids)
+    for k in range(len(grids)):
+        b.set_clock(k, 0.0, 1e30, 5)
+    b.step(5, graph=True)
+    ups = [g.download(want_p=False)[0] for g in grids]
+
+    def recover(batched):
+        for g, up in zip(grids, ups):
+            g.upload(up=up)
+            g.reset_counters()
+        if batched:
+            b.cons_to_prim()
+        else:
+            for g in grids:
+                g.cons_to_prim()
+        return [(*g.download(), g.counters()) for g in grids]
+
+    alone, together = recover(False), recover(True)
+    for k, ((up_a, p_a, c_a), (up_b, p_b, c_b)) in enumerate(zip(alone, together)):
+        assert np.array_equal(up_a, up_b), f"grid {k}: conserved state differs"
+        assert np.array_equal(p_a, p_b), f"grid {k}: primitives differ"
+        assert c_a == c_b, f"grid {k}: counters {c_a} vs {c_b}"
+    b.close()
+    for g in grids:
+        g.close()
+
+
 def test_batch_profile_names():
     s = _stream()
     grids = [_make(pb, s)[0] for pb in (torus_3d(nx=16, ny=8, nz=8), shock_tube(nx=64))]
