@@ -350,6 +350,36 @@ FluxChoice choose_flux(const grhd2_gpu_batch *b, int gi, const Group &grp, const
   return c;
 }
 
+// A scheme group of at least SPLIT_GROUP_CELLS cells over two or more grids runs as two
+// groups of about half the cells each, which a captured step runs as parallel branches of
+// its graph: each half's interface states stay closer to L2 and one half's kernel tails
+// overlap the other's work.  Measured on 32 tori of 400x1x200 run as 1, 2, 4 or 8
+// independent parts on parallel streams: two parts fastest (mixed +3.9 %, FP64 +0.9 %).
+constexpr long long SPLIT_GROUP_CELLS = 2000000;
+void split_large_groups(grhd2_gpu_batch *b, const std::vector<GridDev> &hg) {
+  std::vector<Group> out;
+  for (const Group &grp : b->groups) {
+    long long cells = 0;
+    for (int g : grp.members) cells += hg[g].ncell;
+    if (grp.members.size() < 2 || cells < SPLIT_GROUP_CELLS) {
+      out.push_back(grp);
+      continue;
+    }
+    Group lo = grp, hi = grp;
+    lo.members.clear();
+    hi.members.clear();
+    long long acc = 0;
+    for (int g : grp.members) {  // the first half takes grids until it holds half the cells
+      const bool first = lo.members.empty() || (acc < cells / 2 && grp.members.back() != g);
+      (first ? lo : hi).members.push_back(g);
+      if (first) acc += hg[g].ncell;
+    }
+    out.push_back(lo);
+    out.push_back(hi);
+  }
+  b->groups.swap(out);
+}
+
 // (re)build device descriptors and block maps of a batch
 int build_batch(grhd2_gpu_batch *b) {
   destroy_batch_resources(b);
@@ -370,6 +400,7 @@ int build_batch(grhd2_gpu_batch *b) {
     grp->members.push_back(g);
     grp->cell_dirs = std::max(grp->cell_dirs, 1 + (h->cfg.ny > 1 ? 1 : 0) + (h->cfg.nz > 1 ? 1 : 0));
   }
+  split_large_groups(b, hg);
   // flux variant and tile per scheme group and direction; the tiles go into the batch's
   // copies of the descriptors
   for (int gi = 0; gi < (int)b->groups.size(); ++gi) {

@@ -140,6 +140,36 @@ def test_batch_equals_alone_with_mixed_member():
         g.close()
 
 
+def test_large_group_split_into_parallel_halves():
+    """A scheme group of 2e6 cells or more runs as two halves on parallel graph branches;
+    each grid still gets the result it has alone, bit for bit (two 3D tori of 1.05e6 cells,
+    MP5 + HLLC + sensor, the split kernels and the fused ones)."""
+    s = _stream()
+    pbs = [torus_3d(nx=128, ny=64, nz=128, perturbation_seed=21 + k) for k in range(2)]
+    solo = []
+    for pb in pbs:
+        g, _ = _make(pb, s)
+        g.run(0.0, 1e30, 3)
+        solo.append(g.download(want_p=False)[0])
+        g.close()
+    for variant in ("split", "fused"):
+        grids = [_make(pb, s)[0] for pb in pbs]
+        b = GpuBatch(grids)
+        # the tuner reports one choice per group and direction: two groups of three directions
+        assert len(b.autotune(reps=1)) == 6
+        b.set_flux_variant(variant)
+        for k in range(len(grids)):
+            b.set_clock(k, 0.0, 1e30, 3)
+        b.step(4, graph=True)
+        for k, g in enumerate(grids):
+            assert b.clock(k)[1] == 3
+            up = g.download(want_p=False)[0]
+            assert np.array_equal(up, solo[k]), f"grid {k} differs in the split batch ({variant})"
+        b.close()
+        for g in grids:
+            g.close()
+
+
 def test_batch_cons_to_prim_equals_per_grid():
     """grhd2_gpu_batch_cons_to_prim: every grid's primitives, conserved state and counters
     equal grhd2_gpu_cons_to_prim_all's on the same uploaded state (FP64 grids of six
