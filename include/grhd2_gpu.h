@@ -240,7 +240,10 @@ int grhd2_gpu_set_stream(grhd2_gpu *h, void *stream);
 /* Device bytes a handle of this configuration allocates (for admission by free memory);
  * -1 for an invalid configuration. */
 int64_t grhd2_gpu_device_bytes(const grhd2_gpu_config *cfg);
-/* Group n handles (same device and stream, metric and state uploaded). */
+/* Group n handles (same device and stream, metric and state uploaded).  Grids of one
+ * scheme (precision, reconstruction, Riemann solver) share each kernel launch; a scheme
+ * group of 2e6 cells or more over several grids is run as two halves whose launches are
+ * parallel branches of a step's graph. */
 int grhd2_gpu_batch_create(grhd2_gpu **handles, int n, grhd2_gpu_batch **out);
 /* Set grid k's clock: time t0, final time, and a step limit (< 0: none).  The CFL dt is
  * computed from the grid's metric (update_adaptive_dt). */
@@ -249,7 +252,7 @@ int grhd2_gpu_batch_set_clock(grhd2_gpu_batch *b, int k, double t0, double final
  * graph per step when use_graph != 0).  Asynchronous; grids that finish early stop. */
 int grhd2_gpu_batch_step(grhd2_gpu_batch *b, int nsteps, int use_graph);
 /* grhd2_gpu_cons_to_prim_all of every grid of the batch in one launch per scheme group
- * (same results and counters).  Asynchronous on the batch's stream: for a caller that
+ * (or half group; same results and counters).  Asynchronous on the batch's stream: for a caller that
  * uploads the conserved state of many grids (grhd2_gpu_upload_async) and recovers their
  * primitives before stepping. */
 int grhd2_gpu_batch_cons_to_prim(grhd2_gpu_batch *b);
