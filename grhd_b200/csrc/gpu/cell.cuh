@@ -176,15 +176,24 @@ __device__ __forceinline__ ColMetric<SliceCol<T>> metric_of(const SliceCol<T> &c
 __device__ __forceinline__ bool cell_tile_sliced(const GridDev &G) {
   return G.nz > 1 && G.tiles[TILE_CELL].lx == 5 && G.tiles[TILE_CELL].ly == 0;
 }
-// every thread of the block takes part; columns beyond nx are left unset (no cell reads them)
+// every thread of the block takes part: a thread copies column `lane` of the fields
+// warp, warp + W, ... (W warps in the block), walking both pointers; columns beyond nx are
+// left unset (no cell reads them)
 template <class T>
 __device__ __forceinline__ void stage_slice(T *slice, const T *C, const GridDev &G, unsigned i0, unsigned j) {
-  const long long S = G.nij;
-  const long long col0 = (long long)i0 + (long long)G.nx * j;
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const unsigned ncols = min((unsigned)SLICE_COLS, (unsigned)G.nx - i0);
-  for (unsigned e = threadIdx.x; e < (unsigned)(NCF * SLICE_COLS); e += blockDim.x) {
-    const unsigned fld = e / SLICE_COLS, l = e % SLICE_COLS;
-    if (l < ncols) cp_async<sizeof(T)>(&slice[e], &C[fld * S + col0 + l]);
+  if (lane < ncols) {
+    const T *src = C + ((long long)warp * G.nij + (long long)i0 + (long long)G.nx * j + lane);
+    T *dst = slice + warp * SLICE_COLS + lane;
+    const long long src_step = (long long)nwarps * G.nij;
+    const unsigned dst_step = nwarps * SLICE_COLS;
+#pragma unroll 4
+    for (unsigned fld = warp; fld < (unsigned)NCF; fld += nwarps) {
+      cp_async<sizeof(T)>(dst, src);
+      src += src_step;
+      dst += dst_step;
+    }
   }
   cp_async_commit();
 }
