@@ -1301,4 +1301,66 @@ int grhd2_problem_eval_metric(const grhd2_problem *pb, double x, double y, doubl
   return GRHD2_OK;
 }
 
+namespace {
+// module globals of a metric probe (metric_type, geom_type, use_log_r, bh_mass, a_spin, ny):
+// set directly, without the .par checks, as the reference's set-up tests set them
+bool probe_params(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass, double a_spin,
+                  int32_t ny, Params &P) {
+  if (metric_kind < MINK || metric_kind > KS || geom_kind < CART || geom_kind > SPHEROID || ny < 1) return false;
+  P.metric = metric_kind;
+  P.geom = geom_kind;
+  P.log_r = use_log_r != 0;
+  P.bh_mass = bh_mass;
+  P.a_spin = a_spin;
+  P.ny = ny;
+  return true;
+}
+}  // namespace
+
+int grhd2_host_metric_at(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass, double a_spin,
+                         int32_t ny, double x, double y, double *alpha, double *beta, double *gamma, double *gmunu,
+                         double *det, double *dlnalpha, double *chris, double *dg) {
+  Params P;
+  if (!probe_params(metric_kind, geom_kind, use_log_r, bh_mass, a_spin, ny, P)) return GRHD2_ERR_ARG;
+  MetricOut m;
+  eval_metric(P, x, y, true, m);
+  if (alpha) *alpha = m.alpha;
+  if (beta) std::memcpy(beta, m.beta, sizeof m.beta);
+  if (gamma) std::memcpy(gamma, m.gamma, sizeof m.gamma);
+  if (gmunu) std::memcpy(gmunu, m.gmunu, sizeof m.gmunu);
+  if (det) *det = m.det;
+  if (dlnalpha) std::memcpy(dlnalpha, m.dlna, sizeof m.dlna);
+  if (chris || dg) {
+    double ch[64], d[48];
+    eval_chris_dg(P, x, y, ch, d);
+    if (chris) std::memcpy(chris, ch, sizeof ch);
+    if (dg) std::memcpy(dg, d, sizeof d);
+  }
+  return GRHD2_OK;
+}
+
+int grhd2_host_fm_prepare(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass, double a_spin,
+                          double r_in, double r_max, double *l_ang, double *w_in, int32_t *ok) {
+  Params P;
+  if (!probe_params(metric_kind, geom_kind, use_log_r, bh_mass, a_spin, 1, P) || !l_ang || !w_in || !ok)
+    return GRHD2_ERR_ARG;
+  *ok = fm_prepare(P, r_in, r_max, *l_ang, *w_in) ? 1 : 0;
+  return GRHD2_OK;
+}
+
+int grhd2_host_fm_state(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass, double a_spin,
+                        double adiabatic_index, double rho_floor, double p_floor, double radius, double theta,
+                        double r_in, double K, double l_ang, double w_in, double *state, int32_t *inside) {
+  Params P;
+  if (!probe_params(metric_kind, geom_kind, use_log_r, bh_mass, a_spin, 1, P) || !state || !inside)
+    return GRHD2_ERR_ARG;
+  P.adb = adiabatic_index;
+  P.rho_floor = rho_floor;
+  P.p_floor = p_floor;
+  MetricOut m;
+  eval_metric(P, P.log_r ? std::log(radius) : radius, theta, false, m);
+  *inside = fm_state(P, radius, r_in, K, l_ang, w_in, m.alpha, m.beta, m.gamma, state) ? 1 : 0;
+  return GRHD2_OK;
+}
+
 }  // extern "C"

@@ -62,6 +62,30 @@ int grhd2_problem_eval_metric(const grhd2_problem *pb, double x, double y, doubl
                               double *beta, double *gamma, double *gmunu, double *det,
                               double *dlnalpha, double *chris, double *dg);
 
+/* The same evaluation for any metric kind and geometry (GRHD2_METRIC_*, GRHD2_GEOM_*), with
+ * the module globals metric_type, geom_type, use_log_r, bh_mass, a_spin and ny set directly
+ * and no .par checks -- as the reference's set-up tests set them
+ * (tests/test_minkowski_spherical.f90:19-87 evaluates Eddington-Finkelstein at M = 0).
+ * Replaces set_metric_type + calculate_metric / calculate_christoffel_symbols /
+ * calculate_metric_derivatives (metrics.f90:94-201, :209-1242). */
+int grhd2_host_metric_at(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass,
+                         double a_spin, int32_t ny, double x, double y, double *alpha, double *beta,
+                         double *gamma, double *gmunu, double *det, double *dlnalpha, double *chris,
+                         double *dg);
+/* prepare_fishbone_moncrief (conditions.f90:470-510): the torus's constant specific angular
+ * momentum l and the potential W_in at its inner edge; *ok = 0 where the reference reports
+ * failure. */
+int grhd2_host_fm_prepare(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass,
+                          double a_spin, double r_in, double r_max, double *l_ang, double *w_in,
+                          int32_t *ok);
+/* evaluate_fishbone_moncrief_state (conditions.f90:516-572) at (radius, theta), the metric
+ * evaluated there (radius is mapped to log(radius) on a logarithmic grid): state(5) and
+ * whether the point belongs to the torus (*inside = 0: the floor atmosphere). */
+int grhd2_host_fm_state(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass,
+                        double a_spin, double adiabatic_index, double rho_floor, double p_floor,
+                        double radius, double theta, double r_in, double K, double l_ang, double w_in,
+                        double *state, int32_t *inside);
+
 #ifdef __cplusplus
 }
 #endif
