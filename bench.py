@@ -38,15 +38,18 @@ METRIC = "zone-updates/s per SSP-RK3 step, FP32-mixed vs FP64 at stated L1; serv
 WORKLOAD = "2.5D Kerr-Schild FM torus 400x1x200, WENO5+HLLE, a=0.9, r_in=6, r_max=12, Gamma=4/3"
 
 
+TORUS_KEYS = dict(metric="kerr_schild", geometry="spheroidal", logarithmic_r=True, spin=0.9, bh_mass=1.0,
+                  nx=400, ny=1, nz=200, r_min=1.2, r_max=40.0, theta_min=0, theta_max=1, phi_min=0,
+                  phi_max=2, fm_inner_radius=6.0, fm_pressure_max_radius=12.0,
+                  fm_polytropic_constant=0.0015, adiabatic_index=1.3333333333333333,
+                  reconstruction="weno5", riemann_solver="hlle", shock_sensor=False, cfl=0.4,
+                  perturbation="pressure_noise", perturbation_amplitude=0.01, perturbation_time=0.0,
+                  perturbation_seed=3435)
+
+
 def torus_problem(nx=400, nz=200, seed=3435):
     from grhd_b200.problem import Problem
-    keys = dict(metric="kerr_schild", geometry="spheroidal", logarithmic_r=True, spin=0.9, bh_mass=1.0,
-                nx=nx, ny=1, nz=nz, r_min=1.2, r_max=40.0, theta_min=0, theta_max=1, phi_min=0,
-                phi_max=2, fm_inner_radius=6.0, fm_pressure_max_radius=12.0,
-                fm_polytropic_constant=0.0015, adiabatic_index=1.3333333333333333,
-                reconstruction="weno5", riemann_solver="hlle", shock_sensor=False, cfl=0.4,
-                perturbation="pressure_noise", perturbation_amplitude=0.01, perturbation_time=0.0,
-                perturbation_seed=seed)
+    keys = dict(TORUS_KEYS, nx=nx, nz=nz, perturbation_seed=seed)
     return Problem.from_keys("fishbone_equatorial", **keys)
 
 
@@ -139,12 +142,19 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+STAGE_BYTES_PER_ZONE = {"fp64": 200.0, "mixed": 160.0}
+"""Algorithmic bytes of one cell through one RK stage: read P, u, up and write up, P, five
+values each.  FP64: 5 x 8 x 5 = 200 B.  Mixed policy: P in FP32, u and up in FP64,
+20 + 40 + 40 + 40 + 20 = 160 B.  Face fluxes, interface states, metric tables (k-invariant,
+L2-resident), halo re-reads, ghosts and counters are not algorithmic bytes."""
+STEP_BYTES_PER_ZONE = {k: 3.0 * v for k, v in STAGE_BYTES_PER_ZONE.items()}
+"""Per zone-update (a cell through a full SSP-RK3 step): FP64 600 B, mixed 480 B."""
+
+
 def kernel_bytes(name: str, pb, mixed: bool) -> float:
-    """Algorithmic DRAM bytes of one launch for one grid: each array the kernel must touch,
-    read or written once.  Metric tables (k-invariant, L2-resident) and stencil re-reads
-    are excluded.  recon_d reads P and writes q_L, q_R; riemann_d reads q_L, q_R and writes
-    the face fluxes; cell_update reads the fluxes, P, up and u (or writes u in stage 1) and
-    writes P and up."""
+    """Algorithmic DRAM bytes of one launch for one grid.  The cell update (or a kernel that
+    runs a whole stage) counts the stage's algorithmic bytes, STAGE_BYTES_PER_ZONE per cell;
+    a face kernel counts P read once and what it must write (q_L, q_R or the fluxes)."""
     nx, ny, nz = pb.nx, pb.ny, pb.nz
     n = nx * ny * nz
     ep = 4 if mixed else 8   # primitive / interface / flux element size
@@ -155,16 +165,9 @@ def kernel_bytes(name: str, pb, mixed: bool) -> float:
         return 15 * ep * nf[name[-1]]
     if name.startswith("flux_"):  # fused recon + Riemann: reads P, writes the face fluxes
         return 5 * ep * n + 5 * ep * nf[name[-1]]
-    if name == "cell_update":
-        flux_read = 5 * ep * (nf["x"] + (nf["y"] if ny > 1 else 0) + (nf["z"] if nz > 1 else 0))
-        return flux_read + 2 * 5 * ep * n + 3 * 5 * 8 * n
+    if name in ("cell_update", "stage"):
+        return STAGE_BYTES_PER_ZONE["mixed" if mixed else "fp64"] * n
     return 0.0
-
-
-STEP_BYTES_PER_ZONE = {"fp64": 600.0, "mixed": 600.0}
-"""Algorithmic bytes of one zone-update (a cell through a full SSP-RK3 step): per stage
-read P, u, up, write up, P (5 values each); the mixed policy stores P in FP32 but keeps a
-separate FP64 state, so the same 600 B are counted for both."""
 
 
 # ------------------------------------------------------------------------------------
@@ -371,12 +374,14 @@ def run_ours(args):
                      "step": {"bytes_per_zone_update": STEP_BYTES_PER_ZONE["fp64"],
                               "achieved": STEP_BYTES_PER_ZONE["fp64"] * value / world / 1e9,
                               "frac": STEP_BYTES_PER_ZONE["fp64"] * value / world / 1e9 / peak,
-                              "mixed_achieved": STEP_BYTES_PER_ZONE["mixed"] * mixed_value / world / 1e9}},
+                              "mixed_bytes_per_zone_update": STEP_BYTES_PER_ZONE["mixed"],
+                              "mixed_achieved": STEP_BYTES_PER_ZONE["mixed"] * mixed_value / world / 1e9,
+                              "mixed_frac": STEP_BYTES_PER_ZONE["mixed"] * mixed_value / world / 1e9 / peak}},
     }
     if args.serve_requests > 0:
         out["serve"] = run_serve(args)
     if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(pb, initial_state(pb), max_seconds=args.cpu_seconds)
+        out["cpu_baseline"] = cpu_baseline(max_seconds=args.cpu_seconds)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -404,23 +409,21 @@ def run_serve(args):
     return out
 
 
-def cpu_baseline(pb, p0, max_seconds=15.0, steps=None):
-    """The oracle (plain-C restatement of the reference path) on the host cores."""
-    from oracle.binding import OracleRun, lib
-    o = OracleRun(pb, p0)
-    o.prim_to_cons()
-    o.set_boundary()
-    dt = o.cfl()
-    o.step(dt)  # warm-up
-    n, t0 = 0, time.perf_counter()
-    while True:
-        o.step(dt)
-        n += 1
-        el = time.perf_counter() - t0
-        if (steps is not None and n >= steps) or (steps is None and el >= max_seconds):
-            break
-    return {"value": pb.n_cells * n / el, "unit": "zone-updates/s", "cores": int(lib().orc_num_threads()),
-            "kind": "port", "sample": f"{n} RK3 steps of the {pb.nx}x{pb.ny}x{pb.nz} torus ({el:.1f} s)"}
+def cpu_baseline(max_seconds=15.0, steps=None):
+    """The reference path on the host cores: its restatement in oracle/, built with the
+    reference's own optimisation flags on this host and run on all physical cores with
+    OMP_PROC_BIND=close, in a process of its own (oracle/stopwatch.py)."""
+    cmd = [sys.executable, "-m", "oracle.stopwatch", "run", "--problem", "fishbone_equatorial",
+           "--keys", json.dumps(TORUS_KEYS), "--seconds", str(max_seconds)]
+    if steps is not None:
+        cmd += ["--steps", str(steps)]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"CPU baseline failed: {r.stderr[-2000:]}")
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": d["value"], "unit": "zone-updates/s", "cores": d["threads"], "kind": "port",
+            "sample": f"{d['steps']} RK3 steps of the {d['grid']} torus ({d['seconds']:.1f} s)",
+            "host": d["host"], "flags": d["flags"], "omp": d["omp"], "binary": d["binary"]}
 
 
 def run_reference(args):
@@ -428,15 +431,15 @@ def run_reference(args):
     if rank != 0:
         return
     pb = torus_problem()
-    p0 = initial_state(pb)
-    base = cpu_baseline(pb, p0, steps=args.steps)
+    base = cpu_baseline(steps=args.steps)
     out = {"metric": METRIC, "value": base["value"], "unit": "zone-updates/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": pb.n_cells / base["value"] * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (analytic torus initial data, seeded pressure noise)", "impl": "reference",
            "config": {"workload": WORKLOAD, "nx": pb.nx, "ny": pb.ny, "nz": pb.nz,
-                      "note": "reference Fortran not buildable here (no gfortran); its C restatement (oracle/) "
-                              "timed with all host threads"},
+                      "note": "the reference is Fortran and no Fortran compiler exists on this host or "
+                              "the build host; its C restatement (oracle/) is timed, built with the "
+                              "reference's flags on this host, all physical cores"},
            "cpu_baseline": base,
            "e2e": {"value": base["value"], "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

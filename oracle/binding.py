@@ -16,6 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "libgrhd2_oracle.so")
 # the same oracle calling the C library's exp (as the reference build does) in WENO3
 LIB_LIBM = os.path.join(HERE, "lib", "libgrhd2_oracle_libm.so")
+# the CPU baseline: the same source with the reference's optimisation flags, built on the
+# host that times it (oracle/stopwatch.py); never used to check results
+LIB_STOPWATCH = os.path.join(HERE, "lib", "libgrhd2_oracle_stopwatch.so")
 _dp = C.POINTER(C.c_double)
 
 
@@ -51,9 +54,11 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def lib(libm_exp: bool = False):
-    path = LIB_LIBM if libm_exp else LIB
+def lib(libm_exp: bool = False, stopwatch: bool = False):
+    path = LIB_STOPWATCH if stopwatch else (LIB_LIBM if libm_exp else LIB)
     if path not in _libs:
+        if stopwatch and not os.path.exists(path):
+            raise RuntimeError("the stopwatch build is made on the timing host: python -m oracle.stopwatch")
         if not os.path.exists(path):
             build()
         L = C.CDLL(path)
@@ -124,7 +129,7 @@ def metric_from(mv, bv) -> OrcMetric:
 class OracleRun:
     """Oracle state for one problem: p (ghosted) and up (interior), reference layout."""
 
-    def __init__(self, problem, p=None, libm_exp: bool = False):
+    def __init__(self, problem, p=None, libm_exp: bool = False, stopwatch: bool = False):
         self.problem = problem
         self.cfg = config_from(problem.config(0))
         self._mv = problem.metric_view()
@@ -133,7 +138,7 @@ class OracleRun:
         self.p = (problem.initial_prims() if p is None else p.copy())
         self.up = np.zeros(problem.cons_shape)
         self.counters = OrcCounters()
-        self.L = lib(libm_exp)
+        self.L = lib(libm_exp, stopwatch)
 
     def prim_to_cons(self):
         self.L.orc_prim_to_cons_all(C.byref(self.cfg), C.byref(self.met), _p(self.p), _p(self.up))
