@@ -132,6 +132,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // into shared memory once ([NCF][32], with cp.async) and every thread reads its column
 // from there: ~70 table loads per cell that would otherwise go to L1/L2.
 constexpr int SLICE_COLS = 32;
+static_assert(SLICE_COLS == 32, "stage_slice copies one column per lane of a warp");
 template <class T>
 __host__ __device__ constexpr size_t slice_bytes() { return (size_t)NCF * SLICE_COLS * sizeof(T); }
 template <class T>
@@ -262,12 +263,13 @@ struct PrimSeed {
 // mode is a run-time argument so a persistent kernel needs one copy of the code; the
 // stage kernels pass a constant and the compiler folds it.  The clock has been checked
 // by the caller (dt: the grid's step, 0 in MODE 0).
+// The new primitives go to Pout (the stage kernel's next buffer), or to G.P in place.
 template <class R, class PT, class In>
 __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigned jb, const CellIndex &x, const int MODE,
-                                          double dt, const In &in) {
+                                          double dt, const In &in, PT *Pout = nullptr) {
   const long long c = x.c;
   const Phys P = G.phys;
-  PT *__restrict__ Pio = (PT *)G.P;
+  PT *__restrict__ Pio = Pout ? Pout : (PT *)G.P;
   double *__restrict__ U = G.U;
   double *__restrict__ UP = G.UP;
   double *__restrict__ rhs_out = G.RHS;

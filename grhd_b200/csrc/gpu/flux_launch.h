@@ -39,6 +39,37 @@ void launch_cell(int mode, const GridDev *grids, const BlockMap *map, int nblock
 extern template void launch_cell<double, double>(int, const GridDev *, const BlockMap *, int, int, cudaStream_t);
 extern template void launch_cell<float, float>(int, const GridDev *, const BlockMap *, int, int, cudaStream_t);
 
+// stage kernel (stage.cuh): one whole RK stage (mode 1..3) of 1D grids (sd 0), x-y grids
+// (sd 2) or x-z grids (sd 3); tiles of STAGE_BLOCK cells, one block each
+constexpr int STAGE_BLOCK = 256;
+template <int SD, class R, class PT>
+cudaError_t stage_setup_sd(int rec, int rs);
+template <int SD, class R, class PT>
+void launch_stage_sd(int rec, int rs, int mode, const GridDev *grids, const BlockMap *map, int nblocks, cudaStream_t s);
+#define GRHD_STAGE_EXTERN(SD, R)                                                                            \
+  extern template cudaError_t stage_setup_sd<SD, R, R>(int, int);                                        \
+  extern template void launch_stage_sd<SD, R, R>(int, int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
+GRHD_STAGE_EXTERN(0, double)
+GRHD_STAGE_EXTERN(2, double)
+GRHD_STAGE_EXTERN(3, double)
+GRHD_STAGE_EXTERN(0, float)
+GRHD_STAGE_EXTERN(2, float)
+GRHD_STAGE_EXTERN(3, float)
+#undef GRHD_STAGE_EXTERN
+// sets the kernel's dynamic shared-memory limit; call before the first launch (outside a
+// stream capture)
+template <class R, class PT>
+inline cudaError_t stage_setup(int sd, int rec, int rs) {
+  return sd == 0 ? stage_setup_sd<0, R, PT>(rec, rs) : (sd == 2 ? stage_setup_sd<2, R, PT>(rec, rs) : stage_setup_sd<3, R, PT>(rec, rs));
+}
+template <class R, class PT>
+inline void launch_stage(int sd, int rec, int rs, int mode, const GridDev *grids, const BlockMap *map, int nblocks,
+                         cudaStream_t s) {
+  if (sd == 0) launch_stage_sd<0, R, PT>(rec, rs, mode, grids, map, nblocks, s);
+  else if (sd == 2) launch_stage_sd<2, R, PT>(rec, rs, mode, grids, map, nblocks, s);
+  else launch_stage_sd<3, R, PT>(rec, rs, mode, grids, map, nblocks, s);
+}
+
 // persistent step kernel (persistent.cuh): one contiguous range of items of a phase --
 // the faces of one direction of one grid (dir 1..3) or the cells of one grid (dir 0)
 struct Segment {

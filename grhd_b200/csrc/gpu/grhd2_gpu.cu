@@ -48,12 +48,13 @@ int vfail(std::string &err, int code, const char *fmt, va_list ap) {
 
 // kernel kinds of a step and their items-per-block
 enum Kind {
-  K_RECON_X = 0, K_RIEMANN_X, K_RECON_Y, K_RIEMANN_Y, K_RECON_Z, K_RIEMANN_Z, K_CELL, K_FLUX_X, K_FLUX_Y, K_FLUX_Z, NKIND
+  K_RECON_X = 0, K_RIEMANN_X, K_RECON_Y, K_RIEMANN_Y, K_RECON_Z, K_RIEMANN_Z, K_CELL, K_FLUX_X, K_FLUX_Y, K_FLUX_Z,
+  K_STAGE, NKIND
 };
 const int KIND_BS[NKIND] = {RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, RECON_BS, RIEMANN_BS, CELL_BS,
-                            FUSED_FLUX_BS, FUSED_FLUX_BS, FUSED_FLUX_BS};
+                            FUSED_FLUX_BS, FUSED_FLUX_BS, FUSED_FLUX_BS, STAGE_BLOCK};
 const char *KIND_NAME[NKIND] = {"recon_x", "riemann_x", "recon_y", "riemann_y", "recon_z", "riemann_z",
-                                "cell_update", "flux_x", "flux_y", "flux_z"};
+                                "cell_update", "flux_x", "flux_y", "flux_z", "stage"};
 
 // ---- block tiles ------------------------------------------------------------------------
 unsigned ilog2(unsigned x) {
@@ -102,9 +103,23 @@ long long face_count(const GridDev &G, int dir) {
   return (long long)nI * nJ * nK;
 }
 
+// Tile shape of the stage kernel (stage.cuh) for a grid: 0 for a 1D grid (tiles of 256
+// cells along i), 2 for an x-y grid and 3 for an x-z grid (tiles of 32 x 8 cells); -1 for a
+// 3D grid, which the stage kernel does not cover.
+int stage_sd_of(int ny, int nz) { return ny == 1 ? (nz == 1 ? 0 : 3) : (nz == 1 ? 2 : -1); }
+int stage_sd(const GridDev &G) { return stage_sd_of(G.ny, G.nz); }
+long long stage_tiles(const GridDev &G) {
+  const int sd = stage_sd(G);
+  if (sd < 0) return 0;
+  const int tx = sd == 0 ? STAGE_BLOCK : 32, tr = sd == 0 ? 1 : STAGE_BLOCK / 32;
+  const int nr = sd == 2 ? G.ny : (sd == 3 ? G.nz : 1);
+  return (long long)((G.nx + tx - 1) / tx) * ((nr + tr - 1) / tr);
+}
+
 // threads (tiles x block size) a kernel kind launches for one grid
 long long kind_items(const GridDev &G, int k) {
   if (k == K_CELL) return tile_count(G.tiles[TILE_CELL], LB_CELL, (unsigned)G.nz) * CELL_BS;
+  if (k == K_STAGE) return stage_tiles(G) * STAGE_BLOCK;
   const int dir = k >= K_FLUX_X ? k - K_FLUX_X + 1 : k / 2 + 1;
   if (!dir_active(G, dir)) return 0;
   unsigned nI, nJ, nK;
@@ -153,6 +168,7 @@ struct grhd2_gpu {
 struct Group {
   bool mixed;
   int rec, rs;
+  int sd;  // stage-kernel tile shape of the members (stage_sd_of; -1: 3D grids)
   std::vector<int> members;
   BlockMap *d_map = nullptr;
   int off[NKIND], nb[NKIND];
@@ -165,6 +181,7 @@ struct Group {
   long long n_face = 0, n_cell = 0;
   int max_blocks = 0;  // resident blocks of the group's persistent instantiation
   int cell_dirs = 1;   // the most active directions of a member grid (cell kernel staging)
+  bool stage = false;  // steps run the stage kernel (one launch per stage) instead of face and cell kernels
 };
 
 struct FluxChoice {
@@ -181,6 +198,7 @@ struct grhd2_gpu_batch {
   GridClock *d_clocks = nullptr;  // gathered clocks of every member (grhd2_gpu_batch_clocks)
   std::vector<Group> groups;
   int variant_request = GRHD2_FLUX_AUTO;  // GRHD2_FLUX_AUTO: tuned choice if cached, else the default
+  int stage_request = GRHD2_STAGE_AUTO;   // the stage kernel for groups of 1D and 2D grids
   unsigned tile_request = 0;              // 0: tuned tile if cached, else DEFAULT_TX
   int step_request = GRHD2_STEP_AUTO;     // stage kernels in a graph, or the persistent kernel
   bool persistent = false;                // the mode in use
@@ -350,6 +368,12 @@ FluxChoice choose_flux(const grhd2_gpu_batch *b, int gi, const Group &grp, const
   return c;
 }
 
+// Whether a group's steps run the stage kernel: its grids are 1D or 2D and the request
+// asks for it.
+bool use_stage(const grhd2_gpu_batch *b, const Group &grp) {
+  return grp.sd >= 0 && b->stage_request == GRHD2_STAGE_ON;
+}
+
 // A scheme group of at least SPLIT_GROUP_CELLS cells over two or more grids runs as two
 // groups of about half the cells each, which a captured step runs as parallel branches of
 // its graph: each half's interface states stay closer to L2 and one half's kernel tails
@@ -390,11 +414,12 @@ int build_batch(grhd2_gpu_batch *b) {
   for (int g = 0; g < n; ++g) {
     const grhd2_gpu *h = b->m[g];
     Group *grp = nullptr;
+    const int sd = stage_sd_of(h->cfg.ny, h->cfg.nz);
     for (auto &x : b->groups)
-      if (x.mixed == h->mixed && x.rec == h->cfg.rec_method && x.rs == h->cfg.riemann) grp = &x;
+      if (x.mixed == h->mixed && x.rec == h->cfg.rec_method && x.rs == h->cfg.riemann && x.sd == sd) grp = &x;
     if (!grp) {
-      b->groups.push_back(
-          Group{h->mixed, h->cfg.rec_method, h->cfg.riemann, {}, nullptr, {}, {}, {0, 0, 0}, {DEFAULT_TX, DEFAULT_TX, DEFAULT_TX}});
+      b->groups.push_back(Group{h->mixed, h->cfg.rec_method, h->cfg.riemann, sd, {}, nullptr, {}, {}, {0, 0, 0},
+                                {DEFAULT_TX, DEFAULT_TX, DEFAULT_TX}});
       grp = &b->groups.back();
     }
     grp->members.push_back(g);
@@ -410,6 +435,12 @@ int build_batch(grhd2_gpu_batch *b) {
       grp.variant[d - 1] = ch.variant;
       grp.tx[d - 1] = ch.tx;
       for (int g : grp.members) set_face_tiles(hg[g], d, ch.tx);
+    }
+    grp.stage = use_stage(b, grp);
+    if (grp.stage) {
+      cudaError_t e = grp.mixed ? stage_setup<float, float>(grp.sd, grp.rec, grp.rs)
+                                : stage_setup<double, double>(grp.sd, grp.rec, grp.rs);
+      if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "stage kernel set-up: %s", cudaGetErrorString(e));
     }
   }
   BCUDA_TRY(b, cudaMallocAsync((void **)&b->d_grids, sizeof(GridDev) * n, b->stream));
@@ -510,6 +541,19 @@ int enqueue_cells(grhd2_gpu_batch *b, const Group &grp, cudaStream_t st) {
 // the three SSP-RK3 stages of one scheme group (its grids depend on no other group's)
 int enqueue_group_step(grhd2_gpu_batch *b, const Group &grp, cudaStream_t st) {
   int rc;
+  if (grp.stage) {
+    if (grp.nb[K_STAGE] <= 0) return 0;
+    for (int mode = 1; mode <= 3; ++mode) {
+      if (grp.mixed)
+        launch_stage<float, float>(grp.sd, grp.rec, grp.rs, mode, b->d_grids, grp.d_map + grp.off[K_STAGE],
+                                   grp.nb[K_STAGE], st);
+      else
+        launch_stage<double, double>(grp.sd, grp.rec, grp.rs, mode, b->d_grids, grp.d_map + grp.off[K_STAGE],
+                                     grp.nb[K_STAGE], st);
+      if ((rc = blaunch_check(b, KIND_NAME[K_STAGE]))) return rc;
+    }
+    return 0;
+  }
   if (grp.mixed) {
     if ((rc = enqueue_fluxes<float, float>(b, grp, st)) || (rc = enqueue_cells<1, float, float>(b, grp, st)) ||
         (rc = enqueue_fluxes<float, float>(b, grp, st)) || (rc = enqueue_cells<2, float, float>(b, grp, st)) ||
@@ -732,6 +776,10 @@ long long handle_bytes(const grhd2_gpu_config &c) {
                            (long long)c.nx * c.ny * (c.nz + 1)};
   std::vector<long long> a;
   a.push_back(5 * pplane * es);
+  if (stage_sd_of(c.ny, c.nz) >= 0) {  // P2, P3 of the stage kernel
+    a.push_back(5 * pplane * es);
+    a.push_back(5 * pplane * es);
+  }
   a.push_back(5 * pplane * 8);
   a.push_back(5 * pplane * 8);
   long long nq = nf[0];
@@ -865,6 +913,14 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   char *p = nullptr;
   if ((rc = dalloc(h, &p, 5 * G.pplane * es))) return rc;
   G.P = p;
+  if (stage_sd_of(c.ny, c.nz) >= 0) {  // the stage kernel's primitive rotation (stage.cuh)
+    for (int r = 0; r < 2; ++r) {
+      if ((rc = dalloc(h, &p, 5 * G.pplane * es))) return rc;
+      G.Prot[r] = p;
+    }
+    const int sd = stage_sd_of(c.ny, c.nz);
+    G.stage_ntx = make_fastdiv((unsigned)((c.nx + (sd == 0 ? STAGE_BLOCK : 32) - 1) / (sd == 0 ? STAGE_BLOCK : 32)));
+  }
   if ((rc = dalloc(h, &G.U, 5 * G.pplane))) return rc;
   if ((rc = dalloc(h, &G.UP, 5 * G.pplane))) return rc;
   const long long nf[3] = {(long long)(c.nx + 1) * c.ny * c.nz, (long long)c.nx * (c.ny + 1) * c.nz,
@@ -1701,6 +1757,23 @@ int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant) {
   BCUDA_TRY(b, cudaSetDevice(b->device));
   b->variant_request = variant;
   return build_batch(b);
+}
+
+int grhd2_gpu_batch_set_stage_kernel(grhd2_gpu_batch *b, int mode) {
+  if (!b) return GRHD2_ERR_ARG;
+  if (mode != GRHD2_STAGE_AUTO && mode != GRHD2_STAGE_OFF && mode != GRHD2_STAGE_ON)
+    return bfail(b, GRHD2_ERR_ARG, "invalid stage-kernel mode %d", mode);
+  BCUDA_TRY(b, cudaSetDevice(b->device));
+  b->stage_request = mode;
+  return build_batch(b);
+}
+
+int grhd2_gpu_batch_stage_kernel(grhd2_gpu_batch *b) {
+  if (!b) return GRHD2_ERR_ARG;
+  if (int rc = refresh_batch(b)) return rc;
+  int n = 0;
+  for (const auto &grp : b->groups) n += grp.stage ? 1 : 0;
+  return n;
 }
 
 int grhd2_gpu_batch_set_step_mode(grhd2_gpu_batch *b, int mode) {

@@ -1,0 +1,7 @@
+// stage_fp64_x.cu -- stage kernels of 1D grids, double instantiation (see stage.cuh).
+#include "stage_launch.cuh"
+
+namespace grhd {
+template cudaError_t stage_setup_sd<0, double, double>(int, int);
+template void launch_stage_sd<0, double, double>(int, int, int, const GridDev *, const BlockMap *, int, cudaStream_t);
+}  // namespace grhd

@@ -155,6 +155,8 @@ struct GridDev {
   double dx, dy, dz;
   // the grid's device state
   void *P;                      // primitives (double or float planes)
+  void *Prot[2];                // the stage kernel's rotation buffers P2, P3 (1D and 2D grids; stage.cuh)
+  FastDiv stage_ntx;            // stage-kernel tiles along i
   double *U, *UP, *RHS;         // conserved u, up; RHS scratch of grhd2_gpu_calc_rhs
   void *F[3];                   // face fluxes per direction
   void *Q;                      // interface states of the direction being processed

@@ -130,6 +130,8 @@ GPU_SYMBOLS = {
     "grhd2_gpu_batch_profile_step": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_char_p),
                                                C.c_int, C.POINTER(C.c_int)]),
     "grhd2_gpu_batch_set_flux_variant": (C.c_int, [_VP, C.c_int]),
+    "grhd2_gpu_batch_set_stage_kernel": (C.c_int, [_VP, C.c_int]),
+    "grhd2_gpu_batch_stage_kernel": (C.c_int, [_VP]),
     "grhd2_gpu_batch_clocks": (C.c_int, [_VP, c_double_p, C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
     "grhd2_gpu_set_stream": (C.c_int, [_VP, _VP]),
     "grhd2_gpu_device_bytes": (C.c_int64, [C.POINTER(GpuConfig)]),

@@ -129,6 +129,8 @@ def main(argv=None):
     ap.add_argument("--flux", choices=["auto", "split", "fused", "split_var", "tune"], default="tune",
                     help="face-flux kernel variant ('tune': time variants and tiles on this batch)")
     ap.add_argument("--tile", type=int, default=0, help="face-kernel tile extent along i (0: automatic)")
+    ap.add_argument("--stage", choices=["auto", "on", "off"], default="auto",
+                    help="the stage kernel for 1D and 2D grids (one kernel per RK stage)")
     ap.add_argument("--accuracy", action="store_true",
                     help="run the problem in FP64 and mixed from the same state to --final-time (or --steps) "
                          "and report the mixed-vs-FP64 L1 (and the Michel L1 against the analytic profile)")
@@ -176,6 +178,7 @@ def main(argv=None):
         tuned = None
         batch.set_flux_variant(args.flux)
         batch.set_tile(args.tile)
+    batch.set_stage_kernel(args.stage)
     batch.step(args.warmup, graph=args.graph)
     g.synchronize()
     t0 = time.perf_counter()
@@ -186,7 +189,8 @@ def main(argv=None):
     cells = pb.n_cells * len(grids)
     out = {"cells": cells, "grids": len(grids), "steps": args.steps, "dt": g.cfl(),
            "ms_per_step": el / args.steps * 1e3, "zone_updates_per_s": cells * args.steps / el,
-           "kernels": prof, "counters": g.counters(), "flux_variant": tuned or args.flux}
+           "kernels": prof, "counters": g.counters(), "flux_variant": tuned or args.flux,
+           "stage_groups": batch.stage_groups}
     batch.close()
     for gr in reversed(grids):
         gr.close()

@@ -330,6 +330,22 @@ class GpuBatch:
         """'split' (recon + Riemann kernels), 'fused' (one kernel) or 'auto' (tuned/cached)."""
         self._check(self.lib.grhd2_gpu_batch_set_flux_variant(self._b, self.FLUX_VARIANTS[variant]))
 
+    STAGE_MODES = {"auto": -1, "off": 0, "on": 1}
+
+    def set_stage_kernel(self, mode: str):
+        """'on' (one stage kernel per RK stage for the batch's 1D and 2D grids: every face
+        of a tile and its cell update through shared memory), 'off' (face and cell
+        kernels) or 'auto' (the library's choice)."""
+        self._check(self.lib.grhd2_gpu_batch_set_stage_kernel(self._b, self.STAGE_MODES[mode]))
+
+    @property
+    def stage_groups(self) -> int:
+        """Scheme groups of the batch that step with the stage kernel."""
+        rc = self.lib.grhd2_gpu_batch_stage_kernel(self._b)
+        if rc < 0:
+            self._check(rc)
+        return rc
+
     STEP_MODES = {"auto": -1, "graph": 0, "persistent": 1}
 
     def set_step_mode(self, mode: str):

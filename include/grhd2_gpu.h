@@ -271,6 +271,18 @@ int grhd2_gpu_batch_clocks(grhd2_gpu_batch *b, double *t, int64_t *steps, int *a
 #define GRHD2_FLUX_SPLIT_VAR 2  /* reconstruction kernel (thread per face and variable) + Riemann kernel */
 /* Use one variant for every scheme group and direction of the batch (or AUTO). */
 int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant);
+/* The stage kernel: for grids with at most two active directions (1D, x-y and x-z grids),
+ * one kernel per RK stage computes every face of a tile of cells and the tile's cell
+ * update through shared memory (the primitives with their stencil halo are staged once;
+ * interface states and face fluxes never reach global memory).  Same results and counters
+ * as the face and cell kernels.  No reference counterpart (calc_rhs, the RK combination
+ * and cons_to_prim of grhd2.f90:232-265 in one pass). */
+#define GRHD2_STAGE_AUTO -1  /* the library's choice (currently OFF) */
+#define GRHD2_STAGE_OFF 0    /* face kernels (per the flux variant) and the cell kernel */
+#define GRHD2_STAGE_ON 1     /* the stage kernel where it applies (3D grids keep the face and cell kernels) */
+int grhd2_gpu_batch_set_stage_kernel(grhd2_gpu_batch *b, int mode);
+/* Number of scheme groups of the batch that step with the stage kernel, or a negative error. */
+int grhd2_gpu_batch_stage_kernel(grhd2_gpu_batch *b);
 /* How a batch runs its steps. */
 #define GRHD2_STEP_AUTO -1       /* the library's choice (currently GRAPH, the faster on every size measured) */
 #define GRHD2_STEP_GRAPH 0       /* the stage kernels (recon, Riemann, cell update per stage), one CUDA graph */

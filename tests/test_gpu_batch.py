@@ -41,19 +41,24 @@ def _make(pb, stream, precision="fp64"):
     return g, p0
 
 
-@pytest.mark.parametrize("graph,variant,tile,mode", [
-    (True, "split", 0, "graph"), (False, "split", 128, "graph"), (True, "fused", 0, "graph"),
-    (False, "fused", 64, "graph"), (True, "split", 256, "graph"), (True, "split", 0, "persistent"),
-    (True, "split_var", 0, "graph"), (False, "split_var", 64, "graph")])
-def test_batch_matches_oracle_per_grid(graph, variant, tile, mode):
+@pytest.mark.parametrize("graph,variant,tile,mode,stage", [
+    (True, "split", 0, "graph", "off"), (False, "split", 128, "graph", "off"), (True, "fused", 0, "graph", "off"),
+    (False, "fused", 64, "graph", "off"), (True, "split", 256, "graph", "off"), (True, "split", 0, "persistent", "auto"),
+    (True, "split_var", 0, "graph", "off"), (False, "split_var", 64, "graph", "off"), (True, "split", 0, "graph", "on"),
+    (False, "fused", 0, "graph", "on")])
+def test_batch_matches_oracle_per_grid(graph, variant, tile, mode, stage):
     s = _stream()
     cases = _cases()
     grids, p0s = zip(*[_make(pb, s) for pb, _, _ in cases])
     b = GpuBatch(list(grids))
     b.set_flux_variant(variant)
     b.set_tile(tile)
+    b.set_stage_kernel(stage)
     b.set_step_mode(mode)
     assert b.step_mode == mode
+    if mode == "graph":
+        # every case but the 3D torus is a 1D or 2D grid; scheme groups are per tile shape
+        assert (b.stage_groups > 0) == (stage == "on")
     for k, (pb, tf, ms) in enumerate(cases):
         b.set_clock(k, 0.0, tf, ms)
     # enough replays for the longest grid; finished grids idle
@@ -211,6 +216,7 @@ def test_batch_profile_names():
     b = GpuBatch(grids)
     b.set_step_mode("graph")
     b.set_flux_variant("split")
+    b.set_stage_kernel("off")
     for k in range(2):
         b.set_clock(k, 0.0, 1e30, 1)
     names = [n for n, _ in b.profile_step()]
@@ -219,6 +225,9 @@ def test_batch_profile_names():
     b.set_flux_variant("fused")
     names = [n for n, _ in b.profile_step()]
     assert names.count("flux_x") == 3 * 2 and names.count("flux_z") == 3 and "recon_x" not in names
+    b.set_stage_kernel("on")  # the 1D grid: one stage kernel per stage; the 3D grid keeps its kernels
+    names = [n for n, _ in b.profile_step()]
+    assert names.count("stage") == 3 and names.count("cell_update") == 3 and names.count("flux_x") == 3
     b.set_step_mode("persistent")
     assert [n for n, _ in b.profile_step()] == ["persistent_step"] * 2  # one launch per scheme group
     b.close()
@@ -256,3 +265,86 @@ def test_autotune_leaves_state_and_counters():
     b.close()
     for g in grids:
         g.close()
+
+
+def _stage_cases():
+    """Grids whose tiles end part-way in both directions, grids smaller than one tile, and
+    every tile shape (1D, x-y, x-z), with the shock sensor, HLLC and the two-ghost schemes."""
+    return [
+        shock_tube(nx=5), shock_tube(nx=257, rec="mp5", rs="hllc", sensor=True),
+        shock_tube(nx=300, rec="weno3", rs="hlle", sensor=True), shock_tube(nx=70, rec="tvd", rs="hllc"),
+        shock_tube(nx=64, rec="godunov"), michel(nx=333, rec="weno5", rs="hllc", sensor=True),
+        torus_2p5d(nx=37, nz=11), torus_2p5d(nx=70, nz=30, rec="mp5", rs="hllc", sensor=True),
+        torus_2p5d(nx=20, nz=4, rec="weno3", rs="hlle", sensor=True),
+        shock_tube_xy(nx=33, ny=9), shock_tube_xy(nx=80, ny=20, rec="weno5", rs="hlle", sensor=True),
+    ]
+
+
+def _run_cases(pbs, precision, stage, s, steps=13):
+    grids = [_make(pb, s, precision)[0] for pb in pbs]
+    b = GpuBatch(grids)
+    b.set_stage_kernel(stage)
+    assert (b.stage_groups > 0) == (stage == "on")
+    for k in range(len(grids)):
+        b.set_clock(k, 0.0, 1e30, steps)
+    b.step(5, graph=False)
+    b.step(steps - 5 + 1, graph=True)
+    out = [(g.download(p_template=np.zeros(pb.prim_shape)), g.counters(), b.clock(k))
+           for k, (g, pb) in enumerate(zip(grids, pbs))]
+    b.close()
+    for g in grids:
+        g.close()
+    return out
+
+
+def test_stage_kernel_equals_face_and_cell_kernels():
+    """The stage kernel (every face of a tile and its cell update through shared memory)
+    gives the FP64 state, primitives, clock and all eight counters of the face and cell
+    kernels, bit for bit, on 1D, x-y and x-z grids of awkward sizes."""
+    s = _stream()
+    pbs = _stage_cases()
+    off = _run_cases(pbs, "fp64", "off", s)
+    on = _run_cases(pbs, "fp64", "on", s)
+    for k, pb in enumerate(pbs):
+        (up0, p0), c0, k0 = off[k]
+        (up1, p1), c1, k1 = on[k]
+        assert k0 == k1 and k0[1] == 13, f"case {k}: clocks {k0} {k1}"
+        assert np.array_equal(up0, up1), f"case {k} ({pb.nx}x{pb.ny}x{pb.nz}): state differs"
+        assert np.array_equal(p0, p1), f"case {k}: primitives differ"
+        assert c0 == c1, f"case {k}: counters {c0} vs {c1}"
+
+
+def _stage_cases_mixed():
+    """The shapes of _stage_cases with states the FP32 arithmetic of the mixed policy can
+    represent: the shock tubes at a 10:1 pressure ratio (Sod's states) instead of the
+    1.3e7 of the blast wave, whose 1e-6 right-state pressure is below FP32 round-off of
+    the left state's energy in the fluxes; HLLE on the x-y grids, whose 5 % cell-level
+    pressure noise makes FP32 HLLC fall back to HLLE at other faces than FP64 does (a
+    contact-resolving flux swapped for a diffusive one: relative L1 ~2e-3 on both paths)."""
+    sod = dict(sod_density_left=1.0, sod_pressure_left=1.0, sod_density_right=0.125, sod_pressure_right=0.1)
+    return [
+        shock_tube(nx=5, **sod), shock_tube(nx=257, rec="mp5", rs="hllc", sensor=True, **sod),
+        shock_tube(nx=300, rec="weno3", rs="hlle", sensor=True, **sod), shock_tube(nx=70, rec="tvd", rs="hllc", **sod),
+        michel(nx=333, rec="weno5", rs="hllc", sensor=True),
+        torus_2p5d(nx=37, nz=11), torus_2p5d(nx=70, nz=30, rec="mp5", rs="hllc", sensor=True),
+        torus_2p5d(nx=20, nz=4, rec="weno3", rs="hlle", sensor=True),
+        shock_tube_xy(nx=33, ny=9, rs="hlle", **sod),
+        shock_tube_xy(nx=80, ny=20, rec="weno5", rs="hlle", sensor=True, **sod),
+    ]
+
+
+def test_stage_kernel_mixed_policy_within_bar():
+    """Under the mixed policy the stage kernel and the face and cell kernels are two FP32
+    evaluations (the FP32 units contract to FMA, and which product of a sum is contracted
+    depends on the kernel a function is inlined into): each stays within the policy's bar
+    of the FP64 path, relative L1 per conserved variable at most 1e-5, with the same
+    clocks, on every tile shape."""
+    s = _stream()
+    pbs = _stage_cases_mixed()
+    ref = _run_cases(pbs, "fp64", "on", s)
+    for stage in ("off", "on"):
+        got = _run_cases(pbs, "mixed", stage, s)
+        for k, pb in enumerate(pbs):
+            assert got[k][2] == ref[k][2], f"case {k}: clocks"
+            l1 = rel_l1(got[k][0][0], ref[k][0][0])
+            assert np.all(l1 <= 1e-5), f"stage {stage}, case {k} ({pb.nx}x{pb.ny}x{pb.nz}): relative L1 {l1}"
