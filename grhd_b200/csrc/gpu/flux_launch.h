@@ -40,8 +40,10 @@ extern template void launch_cell<double, double>(int, const GridDev *, const Blo
 extern template void launch_cell<float, float>(int, const GridDev *, const BlockMap *, int, int, cudaStream_t);
 
 // stage kernel (stage.cuh): one whole RK stage (mode 1..3) of 1D grids (sd 0), x-y grids
-// (sd 2) or x-z grids (sd 3); tiles of STAGE_BLOCK cells, one block each
-constexpr int STAGE_BLOCK = 256;
+// (sd 2) or x-z grids (sd 3); tiles of STAGE_TILE_CELLS cells (256 along i, or 32 x 8),
+// one block of STAGE_BLOCK threads each
+constexpr int STAGE_TILE_CELLS = 256;
+constexpr int STAGE_BLOCK = 288;
 template <int SD, class R, class PT>
 cudaError_t stage_setup_sd(int rec, int rs);
 template <int SD, class R, class PT>

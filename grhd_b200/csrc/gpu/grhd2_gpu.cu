@@ -111,7 +111,7 @@ int stage_sd(const GridDev &G) { return stage_sd_of(G.ny, G.nz); }
 long long stage_tiles(const GridDev &G) {
   const int sd = stage_sd(G);
   if (sd < 0) return 0;
-  const int tx = sd == 0 ? STAGE_BLOCK : 32, tr = sd == 0 ? 1 : STAGE_BLOCK / 32;
+  const int tx = sd == 0 ? STAGE_TILE_CELLS : 32, tr = sd == 0 ? 1 : STAGE_TILE_CELLS / 32;
   const int nr = sd == 2 ? G.ny : (sd == 3 ? G.nz : 1);
   return (long long)((G.nx + tx - 1) / tx) * ((nr + tr - 1) / tr);
 }
@@ -369,9 +369,16 @@ FluxChoice choose_flux(const grhd2_gpu_batch *b, int gi, const Group &grp, const
 }
 
 // Whether a group's steps run the stage kernel: its grids are 1D or 2D and the request
-// asks for it.
+// asks for it; AUTO takes it for 1D grids.  Measured on one B200 (the face and cell kernels
+// autotuned or forced to the tuned variant): 64 Michel grids of 1024 cells (MP5 + HLLE,
+// FP64) 5.85e8 zone-updates/s against 4.50e8; 32 tori of 400 x 1 x 200 (WENO5 + HLLE)
+// 5.86e8 against 7.29e8 in FP64 and 1.57e9 against 1.68e9 mixed.  On a 2D tile the stage
+// kernel computes 552 faces for 256 cells (the split kernels 514) at 27 resident warps
+// per SM; on a 1D tile 257 faces, and it saves the launches and the interface-state and
+// flux round trips that dominate small grids.
 bool use_stage(const grhd2_gpu_batch *b, const Group &grp) {
-  return grp.sd >= 0 && b->stage_request == GRHD2_STAGE_ON;
+  if (grp.sd < 0 || b->stage_request == GRHD2_STAGE_OFF) return false;
+  return b->stage_request == GRHD2_STAGE_ON || grp.sd == 0;
 }
 
 // A scheme group of at least SPLIT_GROUP_CELLS cells over two or more grids runs as two
@@ -919,7 +926,8 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
       G.Prot[r] = p;
     }
     const int sd = stage_sd_of(c.ny, c.nz);
-    G.stage_ntx = make_fastdiv((unsigned)((c.nx + (sd == 0 ? STAGE_BLOCK : 32) - 1) / (sd == 0 ? STAGE_BLOCK : 32)));
+    const int tx = sd == 0 ? STAGE_TILE_CELLS : 32;
+    G.stage_ntx = make_fastdiv((unsigned)((c.nx + tx - 1) / tx));
   }
   if ((rc = dalloc(h, &G.U, 5 * G.pplane))) return rc;
   if ((rc = dalloc(h, &G.UP, 5 * G.pplane))) return rc;

@@ -35,14 +35,18 @@
 
 namespace grhd {
 
-constexpr int STAGE_BS = 256;
+// A tile holds STAGE_CELLS cells; its block has STAGE_BS threads, enough that no thread
+// computes more than two of the tile's 552 faces (2D) and no warp waits at the barrier for
+// another's third.
+constexpr int STAGE_CELLS = 256;
+constexpr int STAGE_BS = 288;
 constexpr int STAGE_H = 3;  // halo depth: the widest window (nghost = 3)
 
 // tile geometry per second direction SD: 0 (1D grid), 2 (x-y grid), 3 (x-z grid)
 template <int SD>
 struct StageGeom {
-  static constexpr int TX = SD == 0 ? STAGE_BS : 32;  // cells along i
-  static constexpr int TR = SD == 0 ? 1 : STAGE_BS / 32;  // cells along the second direction
+  static constexpr int TX = SD == 0 ? STAGE_CELLS : 32;  // cells along i
+  static constexpr int TR = SD == 0 ? 1 : STAGE_CELLS / 32;  // cells along the second direction
   static constexpr int BX = TX + 2 * STAGE_H;          // box extent along i
   static constexpr int BR = SD == 0 ? 1 : TR + 2 * STAGE_H;
   static constexpr int NBOX = BX * BR;
@@ -51,6 +55,8 @@ struct StageGeom {
   static constexpr bool SLICE = SD == 3;                // the tile's rows share their (i,j) columns
 };
 static_assert(StageGeom<3>::TX == SLICE_COLS, "x-z tiles stage one table slice of SLICE_COLS columns");
+static_assert(StageGeom<3>::NFX + StageGeom<3>::NFR <= 2 * STAGE_BS && StageGeom<0>::NFX <= STAGE_BS,
+              "at most two faces per thread");
 
 __host__ __device__ constexpr size_t stage_align(size_t b) { return (b + 15) / 16 * 16; }
 template <int SD, class R>
@@ -60,48 +66,62 @@ __host__ __device__ constexpr size_t stage_smem_bytes() {
          stage_align((size_t)NEQ * Gm::NFR * sizeof(R)) + (Gm::SLICE ? slice_bytes<R>() : 0);
 }
 
-// Resident 256-thread blocks per SM the register allocation must allow.
+// Resident blocks per SM the register allocation must allow: 3 (72 registers).  Measured on
+// the 32-grid 2.5D torus batch: the variable loop unrolled (96 or 72 registers), 2 or 4
+// blocks, and x-z tiles without the table slice (4 blocks fit) were 3-21 % slower in FP64
+// and 0-26 % slower (4 blocks: equal) in the mixed policy.
 template <class R>
 constexpr int stage_min_blocks() { return 3; }
 
-// One face of direction DIR whose window cell m (m = 0..5, cells face-2 .. face+3 along
-// DIR) of variable v sits at w[v * vs + m * ms] in shared memory: the interface states
+// One face of direction dir whose window cell m (m = 0..5, cells face-2 .. face+3 along
+// dir) of variable v sits at w[v * vs + m * ms] in shared memory: the interface states
 // with their floors (reconstruction.f90:647-655), then the Riemann flux into out[v * os].
-template <int DIR, int REC, int RS, class R>
-__device__ __forceinline__ void stage_face(const GridDev &G, const Phys &P, const R *w, int vs, int ms, int face,
-                                           int n, long long ft, R *out, int os, bool owned, unsigned &clamps,
-                                           unsigned &fallbacks) {
+// Returns the face's reconstruction floor clamps, plus STAGE_FB if HLLC fell back to HLLE.
+// Out of line, with the variable loop rolled, so the kernel holds one copy of the face
+// code for both directions: with the code of both directions inlined and the variable
+// loop unrolled, the stage kernel stalled on instruction fetch more than on anything else.
+constexpr unsigned STAGE_FB = 1u << 16;
+template <int REC, int RS, class R>
+__device__ __noinline__ unsigned stage_face(const GridDev &G, int dir, const R *w, int vs, int ms, int face, int n,
+                                            long long ft, R *out, int os) {
+  const Phys &P = G.phys;
   int lo, hi;
   stencil_range(REC, P.sensor, lo, hi);
   int br = BR_GODUNOV;
   if (REC != REC_GODUNOV) {
     R rho[5], pr[5];
+    const bool sensor = P.sensor != 0;
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
-      rho[m] = P.sensor ? w[EQ_DE * vs + m * ms] : R(0);
-      pr[m] = P.sensor ? w[EQ_PR * vs + m * ms] : R(0);
+      rho[m] = sensor ? w[EQ_DE * vs + m * ms] : R(0);
+      pr[m] = sensor ? w[EQ_PR * vs + m * ms] : R(0);
     }
-    br = branch_of<REC>(P, rho, pr, face, n, DIR);
+    br = branch_of<REC>(P, rho, pr, face, n, dir);
   }
   R qL[NEQ], qR[NEQ];
   unsigned cl = 0;
   const R rho_fl = R(P.rho_floor), p_fl = R(P.p_floor);
+  const int lim = P.lim;
+  auto one = [&](int v) {
+    R s6[6];
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v) {
-    R s[6];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? w[v * vs + m * ms] : R(0);
-    recon_one<REC>(br, P.lim, s, qL[v], qR[v]);
+    for (int m = 0; m < 6; ++m) s6[m] = (m >= lo && m <= hi) ? w[v * vs + m * ms] : R(0);
+    R l, r;
+    recon_one<REC>(br, lim, s6, l, r);
     if (v == EQ_DE || v == EQ_PR) {  // reconstruction.f90:647-655
       const R fl = v == EQ_DE ? rho_fl : p_fl;
-      cl += (unsigned)!(qL[v] >= fl) + (unsigned)!(qR[v] >= fl);
-      qL[v] = rmax(qL[v], fl);
-      qR[v] = rmax(qR[v], fl);
+      cl += (unsigned)!(l >= fl) + (unsigned)!(r >= fl);
+      l = rmax(l, fl);
+      r = rmax(r, fl);
     }
-  }
+    qL[v] = l;
+    qR[v] = r;
+  };
+#pragma unroll 1
+  for (int v = 0; v < NEQ; ++v) one(v);
   R flux[NEQ];
-  const R *T = face_table<R>(G, DIR - 1);
-  const long long ntab = G.nface[DIR - 1];
+  const R *T = face_table<R>(G, dir - 1);
+  const long long ntab = G.nface[dir - 1];
   bool fb = false;
   if (__ldg(&T[FF_ZERO * ntab + ft]) != R(0)) {  // evolution.f90:69-71, :122-124
 #pragma unroll
@@ -110,18 +130,15 @@ __device__ __forceinline__ void stage_face(const GridDev &G, const Phys &P, cons
     const FaceMetric<R> m = load_face_metric<R>(T, ntab, ft);
     if (RS == RS_HLLC) {
       const FaceFrame<R> fr = load_face_frame<R>(T, ntab, ft);
-      fb = hllc_try(P, qL, qR, DIR, m, fr, flux);
+      fb = hllc_try(P, qL, qR, dir, m, fr, flux);
     } else {
       fb = true;
     }
-    if (fb) hlle(P, qL, qR, DIR, m, flux);
+    if (fb) hlle(P, qL, qR, dir, m, flux);
   }
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) out[v * os] = flux[v];
-  if (owned) {
-    clamps += cl;
-    if (RS == RS_HLLC) fallbacks += fb ? 1u : 0u;
-  }
+  return cl + ((RS == RS_HLLC && fb) ? STAGE_FB : 0u);
 }
 
 // cell_core's inputs for a cell of the tile: its primitives and face fluxes from shared
@@ -158,12 +175,14 @@ __device__ __forceinline__ void stage_buffers(const GridDev &G, int mode, const 
 }
 
 // Batched: block b works on grid map[b].grid, tile map[b].first / STAGE_BS (tiles numbered
-// with i fastest).  mode: the RK stage, 1..3.
+// with i fastest).  mode: the RK stage, 1..3.  The block's first STAGE_CELLS threads
+// update the tile's cells.
 template <int SD, int REC, int RS, class R, class PT>
 __global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
     k_stage(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map, int mode) {
   using Gm = StageGeom<SD>;
   constexpr int TX = Gm::TX, TR = Gm::TR, BX = Gm::BX, NBOX = Gm::NBOX, NFX = Gm::NFX, NFR = Gm::NFR;
+  constexpr bool SLICE = Gm::SLICE;
   constexpr int RD = SD == 0 ? 1 : SD;  // the second direction (1D: none)
   extern __shared__ __align__(16) unsigned char stage_smem[];
   R *s_p = (R *)stage_smem;
@@ -188,7 +207,7 @@ __global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
   const unsigned t = threadIdx.x;
 
   // ---- 1. the primitive box (and the table slice) --------------------------------------
-  if (Gm::SLICE) stage_slice<R>(slice, centre_table<R>(G), G, (unsigned)(i0 - 1), 0u);
+  if (SLICE) stage_slice<R>(slice, centre_table<R>(G), G, (unsigned)(i0 - 1), 0u);
   {
     int lo, hi;
     stencil_range(P.rec, P.sensor, lo, hi);
@@ -216,31 +235,37 @@ __global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
       for (int v = 0; v < NEQ; ++v) s_p[v * NBOX + pos] = R(q[v]);
     }
   }
-  if (Gm::SLICE) cp_async_wait<0>();
+  if (SLICE) cp_async_wait<0>();
   __syncthreads();
 
-  // ---- 2. the faces of the tile ----------------------------------------------------------
+  // ---- 2. the faces of the tile: x faces, then those of the second direction ------------
   unsigned clamps = 0, fallbacks = 0;
   {
     const int afx = min(TX, nx - i0 + 1);  // last x face of the tile (local index)
-    for (int q = (int)t; q < NFX; q += STAGE_BS) {
-      const int rr = q / (TX + 1), a = q - rr * (TX + 1);
-      const int f = i0 - 1 + a, rc = r0 + rr;
-      if (a > afx || rc > nr) continue;
-      const int j = SD == 2 ? rc : 1;
-      const long long ft = (long long)f + (long long)(nx + 1) * (j - 1);
-      stage_face<1, REC, RS, R>(G, P, s_p + (rr + (SD == 0 ? 0 : STAGE_H)) * BX + a, NBOX, 1, f, nx, ft, s_fx + q, NFX,
-                                a < TX || f == nx, clamps, fallbacks);
-    }
-    if (SD != 0) {
-      const int afr = min(TR, nr - r0 + 1);
-      for (int q = (int)t; q < NFR; q += STAGE_BS) {
-        const int b = q / TX, a = q - b * TX;
+    const int afr = min(TR, nr - r0 + 1);  // last face of the second direction (local index)
+    for (int q = (int)t; q < NFX + NFR; q += STAGE_BS) {
+      unsigned res;
+      bool owned;
+      if (q < NFX) {
+        const int rr = q / (TX + 1), a = q - rr * (TX + 1);
+        const int f = i0 - 1 + a, rc = r0 + rr;
+        if (a > afx || rc > nr) continue;
+        const int j = SD == 2 ? rc : 1;
+        const long long ft = (long long)f + (long long)(nx + 1) * (j - 1);
+        res = stage_face<REC, RS, R>(G, 1, s_p + (rr + (SD == 0 ? 0 : STAGE_H)) * BX + a, NBOX, 1, f, nx, ft, s_fx + q,
+                                     NFX);
+        owned = a < TX || f == nx;
+      } else {
+        const int qr = q - NFX, b = qr / TX, a = qr - b * TX;
         const int f = r0 - 1 + b, i = i0 + a;
         if (i > nx || b > afr) continue;
         const long long ft = SD == 3 ? (long long)(i - 1) : (long long)(i - 1) + (long long)nx * f;
-        stage_face<RD, REC, RS, R>(G, P, s_p + b * BX + a + STAGE_H, NBOX, BX, f, nr, ft, s_fr + q, NFR,
-                                   b < TR || f == nr, clamps, fallbacks);
+        res = stage_face<REC, RS, R>(G, RD, s_p + b * BX + a + STAGE_H, NBOX, BX, f, nr, ft, s_fr + qr, NFR);
+        owned = b < TR || f == nr;
+      }
+      if (owned) {
+        clamps += res & (STAGE_FB - 1u);
+        fallbacks += res >> 16;
       }
     }
   }
@@ -249,6 +274,7 @@ __global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
   __syncthreads();
 
   // ---- 3. the cells of the tile ----------------------------------------------------------
+  if (t >= (unsigned)STAGE_CELLS) return;
   const int a = (int)(t % TX), rr = (int)(t / TX);
   const int i = i0 + a, r = r0 + rr;
   if (i > nx || r > nr) return;
@@ -258,7 +284,7 @@ __global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
   const R *sp = s_p + (rr + (SD == 0 ? 0 : STAGE_H)) * BX + a + STAGE_H;
   const R *sfx = s_fx + rr * (TX + 1) + a;
   const R *sfr = s_fr + rr * TX + a;
-  if constexpr (Gm::SLICE) {
+  if constexpr (SLICE) {
     if constexpr (sizeof(PT) == sizeof(float)) {  // mixed: FP32 slice for the sources, FP64 con2prim metric from global
       const TileIn<R, PT, SD, SliceCol<R>, LazyCol<double>> in{G, x, sp, sfx, sfr, SliceCol<R>{slice, (unsigned)a},
                                                              LazyCol<double>{global_col(G.centre, G, ij)}};

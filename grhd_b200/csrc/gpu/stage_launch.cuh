@@ -8,7 +8,7 @@
 
 namespace grhd {
 
-static_assert(STAGE_BS == STAGE_BLOCK, "the launchers' block size is the kernel's tile size");
+static_assert(STAGE_BS == STAGE_BLOCK && STAGE_CELLS == STAGE_TILE_CELLS, "the host's tile geometry is the kernel's");
 
 template <int SD, int REC, class R, class PT>
 inline const void *stage_fn(int rs) {

@@ -277,7 +277,8 @@ int grhd2_gpu_batch_set_flux_variant(grhd2_gpu_batch *b, int variant);
  * interface states and face fluxes never reach global memory).  Same results and counters
  * as the face and cell kernels.  No reference counterpart (calc_rhs, the RK combination
  * and cons_to_prim of grhd2.f90:232-265 in one pass). */
-#define GRHD2_STAGE_AUTO -1  /* the library's choice (currently OFF) */
+#define GRHD2_STAGE_AUTO -1  /* the library's choice: the stage kernel for 1D grids (faster there), the
+                                face and cell kernels for 2D grids */
 #define GRHD2_STAGE_OFF 0    /* face kernels (per the flux variant) and the cell kernel */
 #define GRHD2_STAGE_ON 1     /* the stage kernel where it applies (3D grids keep the face and cell kernels) */
 int grhd2_gpu_batch_set_stage_kernel(grhd2_gpu_batch *b, int mode);
