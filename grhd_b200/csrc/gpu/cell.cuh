@@ -24,12 +24,20 @@ __device__ __forceinline__ GlobalCol<T> global_col(const T *C, const GridDev &G,
 // ------------------------------------------------------------------------------------
 // calc_sources (equations.f90:509-552) + calculate_stress_energy_tensor (metrics.f90:1251)
 // ------------------------------------------------------------------------------------
+// Under the mixed policy (R = float) the contraction of T^{mu nu} with the metric
+// derivatives runs in FP32, while the lapse and sqrt(gamma) factors -- the time component
+// of the four-velocity W / alpha and the closing alpha sqrt(gamma) (alpha) scaling of
+// equations.f90:550-551, which grow steep near the horizon -- are applied in FP64 from the
+// FP64 centre table (alpha64, sqg64) in every cell.  The result is FP64 in both policies.
 template <class R, class Col>
-__device__ __forceinline__ void sources(const Phys &P, const Col &col, const double (&qd)[NEQ], R (&src)[NEQ]) {
+__device__ __forceinline__ void sources(const Phys &P, const Col &col, const double (&qd)[NEQ], double (&out)[NEQ],
+                                        double alpha64, double sqg64) {
 #pragma unroll
-  for (int n = 0; n < NEQ; ++n) src[n] = R(0);
+  for (int n = 0; n < NEQ; ++n) out[n] = 0.0;
   if (P.srhd) return;
   auto ld = [&](int fld) { return R(col(fld)); };
+  constexpr bool mixed = sizeof(R) == sizeof(float);
+  R src[NEQ];
   const R alpha = ld(CF_ALPHA), sqg = ld(CF_SQG);
   FaceMetric<R> m;
   m.g11 = ld(CF_G11); m.g12 = ld(CF_G12); m.g13 = ld(CF_G13); m.g22 = ld(CF_G22); m.g23 = ld(CF_G23); m.g33 = ld(CF_G33);
@@ -41,7 +49,7 @@ __device__ __forceinline__ void sources(const Phys &P, const Col &col, const dou
   const R h = R(1) + R(P.g1) * q[EQ_PR] / q[EQ_DE];
   const R W = R(1) / sqrt(R(1) - vsq);
   R uf[4];
-  uf[0] = W / alpha;
+  uf[0] = mixed ? R((double)W / alpha64) : W / alpha;
   uf[1] = W * (v[0] - ld(CF_VA));  // beta^i / alpha: per (i,j), rounded once (the same quotient)
   uf[2] = W * (v[1] - ld(CF_VA + 1));
   uf[3] = W * (v[2] - ld(CF_VA + 2));
@@ -68,9 +76,17 @@ __device__ __forceinline__ void sources(const Phys &P, const Col &col, const dou
     for (int nu = 0; nu <= 3; ++nu) st = st - T[sym4(mu, nu)] * ld(CF_CH0 + sym4(mu, nu));
   }
   src[EQ_PR] = st;
+  if constexpr (mixed) {
 #pragma unroll
-  for (int n = 0; n < NEQ; ++n) src[n] = src[n] * alpha * sqg;
-  src[EQ_PR] = src[EQ_PR] * alpha;
+    for (int n = 0; n < NEQ; ++n) out[n] = (double)src[n] * alpha64 * sqg64;
+    out[EQ_PR] = out[EQ_PR] * alpha64;
+  } else {
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) src[n] = src[n] * alpha * sqg;
+    src[EQ_PR] = src[EQ_PR] * alpha;
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) out[n] = (double)src[n];
+  }
 }
 
 template <class Col>
@@ -263,6 +279,72 @@ struct PrimSeed {
 // mode is a run-time argument so a persistent kernel needs one copy of the code; the
 // stage kernels pass a constant and the compiler folds it.  The clock has been checked
 // by the caller (dt: the grid's step, 0 in MODE 0).
+// ---- compensated RK3 accumulation (mixed policy with carries) ------------------------
+// The state is a double-double: up + carry (and u + carry), the carry holding what the FP64
+// rounding of each stage combination dropped.  Error-free transformations: Knuth's TwoSum
+// (s = a + b exactly as s + e) and the FMA form of the exact product (p + e = a b).
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+// (ah, al) + (bh, bl), renormalised so that |l| <= ulp(h) / 2
+__device__ __forceinline__ void dd_add(double ah, double al, double bh, double bl, double &h, double &l) {
+  double s, e;
+  two_sum(ah, bh, s, e);
+  e = e + (al + bl);
+  h = s + e;
+  l = e - (h - s);
+}
+// (ah, al) * b
+__device__ __forceinline__ void dd_mul(double ah, double al, double b, double &h, double &l) {
+  const double p = ah * b;
+  const double e = fma(ah, b, -p) + al * b;
+  h = p + e;
+  l = e - (h - p);
+}
+__device__ __forceinline__ double load_carry(const GridDev &G, const void *C, long long i) {
+  return G.carry == 1 ? ((const double *)C)[i] : (double)((const float *)C)[i];
+}
+__device__ __forceinline__ void store_carry(const GridDev &G, void *C, long long i, double x) {
+  if (G.carry == 1) ((double *)C)[i] = x;
+  else ((float *)C)[i] = (float)x;
+}
+// The SSP-RK3 combination of grhd2.f90:243-249 in double-double arithmetic: rhs*dt with its
+// rounding error, up + rhs*dt, then u = up (stage 1), 0.75 u + 0.25 (...) (stage 2) or
+// (u + 2 (...)) / 3 (stage 3).  hi goes to con2prim as the stage's FP64 state, lo to the
+// carry.
+template <class In>
+__device__ __forceinline__ void rk_stage_compensated(const GridDev &G, long long c, int MODE, double dt, const In &in,
+                                                     const double (&rhs)[NEQ], double (&hi)[NEQ], double (&lo)[NEQ]) {
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) {
+    const long long k = v * G.pplane + c;
+    const double up = in.up(v), upl = load_carry(G, G.UPc, k);
+    const double d = rhs[v] * dt, dl = fma(rhs[v], dt, -d);
+    double th, tl;
+    dd_add(up, upl, d, dl, th, tl);  // up + rhs*dt
+    if (MODE == 1) {
+      G.U[k] = up;  // u = up (grhd2.f90:232), carry included
+      store_carry(G, G.Uc, k, upl);
+      hi[v] = th;
+      lo[v] = tl;
+    } else if (MODE == 2) {
+      double ah, al, bh, bl;
+      dd_mul(in.u(v), load_carry(G, G.Uc, k), 0.75, ah, al);
+      dd_mul(th, tl, 0.25, bh, bl);
+      dd_add(ah, al, bh, bl, hi[v], lo[v]);
+    } else {
+      double sh, sl;
+      dd_add(in.u(v), load_carry(G, G.Uc, k), 2.0 * th, 2.0 * tl, sh, sl);
+      const double q = sh / 3.0;
+      const double ql = (fma(-q, 3.0, sh) + sl) / 3.0;
+      hi[v] = q + ql;
+      lo[v] = ql - (hi[v] - q);
+    }
+  }
+}
+
 // The new primitives go to Pout (the stage kernel's next buffer), or to G.P in place.
 template <class R, class PT, class In>
 __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigned jb, const CellIndex &x, const int MODE,
@@ -279,9 +361,14 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
   double q[NEQ];
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) q[v] = in.prim(v);
-  R src[NEQ];
-  sources<R>(P, in.table_r(), q, src);
+  double src[NEQ];
+  if constexpr (sizeof(R) == sizeof(float))
+    sources<R>(P, in.table_r(), q, src, in.table64()(CF_ALPHA), in.table64()(CF_SQG));
+  else
+    sources<R>(P, in.table_r(), q, src, 0.0, 0.0);
   in.wait_fluxes();
+  // the flux differences in R; their sum with the (FP64) sources in FP64 (for R = double
+  // the reference's order: -(F_i - F_{i-1})/dx + S, then - (G_j - G_{j-1})/dy, ...)
   double rhs[NEQ];
 #pragma unroll
   for (int v = 0; v < NEQ; ++v) {
@@ -292,14 +379,14 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
       const R a = in.flux(1, 1, v), b = in.flux(1, 0, v);
-      rhs[v] = (double)(R(rhs[v]) - div_pos(a - b, R(dy)));
+      rhs[v] = rhs[v] - (double)div_pos(a - b, R(dy));
     }
   }
   if (G.nz > 1) {
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
       const R a = in.flux(2, 1, v), b = in.flux(2, 0, v);
-      rhs[v] = (double)(R(rhs[v]) - div_pos(a - b, R(dz)));
+      rhs[v] = rhs[v] - (double)div_pos(a - b, R(dz));
     }
   }
   if (MODE == 0) {
@@ -309,24 +396,34 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
   }
   in.wait_state();
   double cs[NEQ];
+  constexpr bool mixed = sizeof(PT) == sizeof(float);
+  const bool comp = mixed && G.carry != 0;  // compensated accumulation (mixed policy only)
+  double lo[NEQ];
+  if (comp) {
+    rk_stage_compensated(G, c, MODE, dt, in, rhs, cs, lo);
+  } else {
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v) {
-    const double up = in.up(v);
-    double nv;
-    if (MODE == 1) {
-      U[v * G.pplane + c] = up;  // u = up (grhd2.f90:232)
-      nv = up + rhs[v] * dt;
-    } else if (MODE == 2) {
-      nv = 0.75 * in.u(v) + 0.25 * (up + rhs[v] * dt);
-    } else {
-      nv = (in.u(v) + 2.0 * (up + rhs[v] * dt)) / 3.0;
+    for (int v = 0; v < NEQ; ++v) {
+      const double up = in.up(v);
+      double nv;
+      if (MODE == 1) {
+        U[v * G.pplane + c] = up;  // u = up (grhd2.f90:232)
+        nv = up + rhs[v] * dt;
+      } else if (MODE == 2) {
+        nv = 0.75 * in.u(v) + 0.25 * (up + rhs[v] * dt);
+      } else {
+        nv = (in.u(v) + 2.0 * (up + rhs[v] * dt)) / 3.0;
+      }
+      cs[v] = nv;
     }
-    cs[v] = nv;
   }
+  double hi[NEQ];
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) hi[v] = cs[v];
   const auto cm = metric_of(in.table64());
   double pr[NEQ];
   unsigned fl;
-  if constexpr (sizeof(PT) == sizeof(float))  // mixed policy: the seeded root finder
+  if constexpr (mixed)  // mixed policy: the seeded root finder
     fl = cons_to_prim(P, cm, cs, pr, PrimSeed<In, decltype(cm)>{in, cm});
   else
     fl = cons_to_prim(P, cm, cs, pr);
@@ -334,6 +431,10 @@ __device__ __forceinline__ void cell_core(const GridDev &G, unsigned ia, unsigne
   for (int v = 0; v < NEQ; ++v) {
     UP[v * G.pplane + c] = cs[v];
     Pio[v * G.pplane + c] = (PT)pr[v];
+  }
+  if (comp) {  // a value con2prim changed (floors, causal rescaling) starts without a carry
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) store_carry(G, G.UPc, v * G.pplane + c, cs[v] == hi[v] ? lo[v] : 0.0);
   }
   c2p_count(cnt, fl);
 }

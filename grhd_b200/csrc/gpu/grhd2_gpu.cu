@@ -706,6 +706,16 @@ int self_batch(grhd2_gpu *h) {
   return 0;
 }
 
+// The compensated accumulation's carries restart at zero whenever up is written outside a
+// step (upload, prim_to_cons, cons_to_prim's floors): the state is then up alone.
+int clear_carries(grhd2_gpu *h, cudaStream_t st) {
+  if (!h->G.carry) return 0;
+  const size_t cb = (h->G.carry == 1 ? sizeof(double) : sizeof(float)) * 5 * (size_t)h->G.pplane;
+  CUDA_TRY(h, cudaMemsetAsync(h->G.Uc, 0, cb, st));
+  CUDA_TRY(h, cudaMemsetAsync(h->G.UPc, 0, cb, st));
+  return 0;
+}
+
 int write_clock(grhd2_gpu *h) {
   CUDA_TRY(h, cudaMemcpyAsync(h->G.clock, &h->hclock, sizeof(GridClock), cudaMemcpyHostToDevice, h->stream));
   return 0;
@@ -777,7 +787,7 @@ size_t diag_bytes(int nx, int ny, int nz) {
 // device bytes a handle of this configuration allocates (create + set_metric + set_bc_data;
 // the calc_rhs scratch is not counted), each allocation rounded up to 4 KB
 long long handle_bytes(const grhd2_gpu_config &c) {
-  const long long es = c.precision_policy == GRHD2_PREC_MIXED ? 4 : 8;
+  const long long es = c.precision_policy != GRHD2_PREC_FP64 ? 4 : 8;
   const long long ncell = (long long)c.nx * c.ny * c.nz, pplane = (ncell + 31) / 32 * 32;
   const long long nf[3] = {(long long)(c.nx + 1) * c.ny * c.nz, (long long)c.nx * (c.ny + 1) * c.nz,
                            (long long)c.nx * c.ny * (c.nz + 1)};
@@ -789,6 +799,11 @@ long long handle_bytes(const grhd2_gpu_config &c) {
   }
   a.push_back(5 * pplane * 8);
   a.push_back(5 * pplane * 8);
+  if (c.precision_policy == GRHD2_PREC_MIXED_COMP64 || c.precision_policy == GRHD2_PREC_MIXED_COMP32) {
+    const long long cb = c.precision_policy == GRHD2_PREC_MIXED_COMP64 ? 8 : 4;  // carries of u and up
+    a.push_back(5 * pplane * cb);
+    a.push_back(5 * pplane * cb);
+  }
   long long nq = nf[0];
   for (int d = 0; d < 3; ++d) {
     if ((d == 1 && c.ny == 1) || (d == 2 && c.nz == 1)) continue;
@@ -806,7 +821,7 @@ long long handle_bytes(const grhd2_gpu_config &c) {
     a.push_back(5LL * c.nx * c.nz * 8);
     a.push_back(5LL * c.nx * c.ny * 8);
   }
-  for (long long tb : {8LL, c.precision_policy == GRHD2_PREC_MIXED ? 4LL : 0LL}) {  // tables (+ FP32 copies)
+  for (long long tb : {8LL, c.precision_policy != GRHD2_PREC_FP64 ? 4LL : 0LL}) {  // tables (+ FP32 copies)
     if (tb == 0) continue;
     a.push_back((long long)NCF * c.nx * c.ny * tb);
     a.push_back((long long)NFF * (c.nx + 1) * c.ny * tb);
@@ -874,7 +889,7 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   if (c.riemann != 1 && c.riemann != 2) return fail(h, GRHD2_ERR_ARG, "riemann solver id %d unsupported (1 HLLE, 2 HLLC)", c.riemann);
   if (c.case_id < 1 || c.case_id > 12) return fail(h, GRHD2_ERR_ARG, "invalid case id %d", c.case_id);
   if (c.metric_kind < 0 || c.metric_kind > 2 || c.geom_kind < 0 || c.geom_kind > 3) return fail(h, GRHD2_ERR_ARG, "invalid metric/geometry id");
-  if (c.precision_policy != GRHD2_PREC_FP64 && c.precision_policy != GRHD2_PREC_MIXED)
+  if (c.precision_policy < GRHD2_PREC_FP64 || c.precision_policy > GRHD2_PREC_MIXED_COMP32)
     return fail(h, GRHD2_ERR_ARG, "invalid precision policy %d", c.precision_policy);
   if (c.case_id == 12 && (c.nz % 2) != 0) return fail(h, GRHD2_ERR_BOUNDARY, "nz must be even for 3D trans-polar boundary conditions");
   if ((c.case_id == 11 || c.case_id == 12) && c.ny < c.nghost)
@@ -886,7 +901,7 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
       (long long)c.nx * c.ny * (c.nz + 1) > 2000000000LL)
     return fail(h, GRHD2_ERR_ARG, "grid too large (face count must stay below 2e9)");
 
-  h->mixed = c.precision_policy == GRHD2_PREC_MIXED;
+  h->mixed = c.precision_policy != GRHD2_PREC_FP64;
   GridDev &G = h->G;
   Phys &ph = G.phys;
   ph.rec = c.rec_method; ph.lim = c.tvd_limiter; ph.rs = c.riemann; ph.sensor = c.shock_sensor ? 1 : 0;
@@ -931,6 +946,15 @@ int grhd2_gpu_create_on_stream(const grhd2_gpu_config *cfg, void *stream, grhd2_
   }
   if ((rc = dalloc(h, &G.U, 5 * G.pplane))) return rc;
   if ((rc = dalloc(h, &G.UP, 5 * G.pplane))) return rc;
+  G.carry = c.precision_policy == GRHD2_PREC_MIXED_COMP64 ? 1 : (c.precision_policy == GRHD2_PREC_MIXED_COMP32 ? 2 : 0);
+  if (G.carry) {  // carries of u and up, starting at zero
+    const size_t cb = G.carry == 1 ? sizeof(double) : sizeof(float);
+    for (void **cp : {&G.Uc, &G.UPc}) {
+      if ((rc = dalloc(h, &p, 5 * G.pplane * cb))) return rc;
+      CUDA_TRY(h, cudaMemsetAsync(p, 0, 5 * G.pplane * cb, h->stream));
+      *cp = p;
+    }
+  }
   const long long nf[3] = {(long long)(c.nx + 1) * c.ny * c.nz, (long long)c.nx * (c.ny + 1) * c.nz,
                            (long long)c.nx * c.ny * (c.nz + 1)};
   long long nq = nf[0];
@@ -1113,8 +1137,9 @@ static int upload_impl(grhd2_gpu *h, const double *up, const double *p, bool syn
   }
   if (up) {
     CUDA_TRY(h, cudaMemcpyAsync(h->staging, up, h->n_interior * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    k_cons_in<<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, h->staging, G.UP);
+    k_cons_in<<<nblocks(G.ncell, LAYOUT_BS), LAYOUT_BS, 0, h->stream>>>(G, h->staging, G.UP);
     if (int rc = launch_check(h)) return rc;
+    if (int rc = clear_carries(h, h->stream)) return rc;
     h->cons_set = true;
   }
   if (sync) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -1131,6 +1156,7 @@ int grhd2_gpu_prim_to_cons_all(grhd2_gpu *h) {
   if (h->mixed) k_p2c_all<float><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (const float *)G.P, G.UP);
   else k_p2c_all<double><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (const double *)G.P, G.UP);
   if (int rc = launch_check(h)) return rc;
+  if (int rc = clear_carries(h, h->stream)) return rc;
   h->cons_set = true;
   return GRHD2_OK;
 }
@@ -1221,7 +1247,7 @@ int grhd2_gpu_calc_rhs(grhd2_gpu *h, double *rhs_host) {
     if (rc) return fail(h, rc, "%s", b->err.c_str());
   }
   if (rhs_host) {
-    k_cons_out<<<nblocks(h->G.ncell, 256), 256, 0, h->stream>>>(h->G, h->G.RHS, h->staging);
+    k_cons_out<<<nblocks(h->G.ncell, LAYOUT_BS), LAYOUT_BS, 0, h->stream>>>(h->G, h->G.RHS, h->staging);
     if ((rc = launch_check(h))) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(rhs_host, h->staging, h->n_interior * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   }
@@ -1236,6 +1262,7 @@ int grhd2_gpu_cons_to_prim_all(grhd2_gpu *h) {
   if (h->mixed) k_c2p_all<float><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (float *)G.P, G.UP, G.cnt);
   else k_c2p_all<double><<<nblocks(G.ncell, 128), 128, 0, h->stream>>>(G, G.phys, (double *)G.P, G.UP, G.cnt);
   if (int rc = launch_check(h)) return rc;
+  if (int rc = clear_carries(h, h->stream)) return rc;
   h->prims_set = true;
   return GRHD2_OK;
 }
@@ -1261,7 +1288,7 @@ static int download_impl(grhd2_gpu *h, double *up, double *p, bool sync) {
   }
   if (up) {
     if (!h->cons_set) return fail(h, GRHD2_ERR_STATE, "conserved state not uploaded");
-    k_cons_out<<<nblocks(G.ncell, 256), 256, 0, h->stream>>>(G, G.UP, h->staging);
+    k_cons_out<<<nblocks(G.ncell, LAYOUT_BS), LAYOUT_BS, 0, h->stream>>>(G, G.UP, h->staging);
     if (int rc = launch_check(h)) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(up, h->staging, h->n_interior * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   }
@@ -1305,25 +1332,31 @@ static int faces_common(grhd2_gpu *h, int n, int dir, const double *qL, const do
   CUDA_TRY(h, cudaSetDevice(h->device));
   std::vector<double> T;
   if (int rc = build_face_table(h, T, (size_t)n, dir, alpha, beta, gamma, sqg, {})) return rc;
+  // scratch of this call only, from the device's stream-ordered pool on the handle's
+  // stream (no device-wide synchronisation), released after the result is copied out
   double *dT = nullptr, *dq = nullptr;
-  // scratch of this call only, on the legacy stream like the copies below
-  if (cudaMalloc((void **)&dT, T.size() * sizeof(double)) != cudaSuccess)
-    return fail(h, GRHD2_ERR_NOMEM, "cudaMalloc of the face table failed");
-  if (cudaMalloc((void **)&dq, (size_t)15 * n * sizeof(double)) != cudaSuccess) {
-    cudaFree(dT);
-    return fail(h, GRHD2_ERR_NOMEM, "cudaMalloc of the face states failed");
+  cudaStream_t st = h->stream;
+  CUDA_TRY(h, cudaMallocAsync((void **)&dT, T.size() * sizeof(double), st));
+  cudaError_t e = cudaMallocAsync((void **)&dq, (size_t)15 * n * sizeof(double), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dT, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dq, qL, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && qR)
+    e = cudaMemcpyAsync(dq + 5 * n, qR, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    if (h->mixed)
+      k_riemann_faces<float><<<nblocks(n, 128), 128, 0, st>>>(h->G.phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n,
+                                                              physical_only);
+    else
+      k_riemann_faces<double><<<nblocks(n, 128), 128, 0, st>>>(h->G.phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n,
+                                                               physical_only);
+    e = cudaGetLastError();
   }
-  cudaMemcpy(dT, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice);
-  cudaMemcpy(dq, qL, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice);
-  if (qR) cudaMemcpy(dq + 5 * n, qR, (size_t)5 * n * sizeof(double), cudaMemcpyHostToDevice);
-  if (h->mixed)
-    k_riemann_faces<float><<<nblocks(n, 128), 128>>>(h->G.phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n, physical_only);
-  else
-    k_riemann_faces<double><<<nblocks(n, 128), 128>>>(h->G.phys, n, dir, dq, dq + 5 * n, dT, dq + 10 * n, physical_only);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpy(flux, dq + 10 * n, (size_t)5 * n * sizeof(double), cudaMemcpyDeviceToHost);
-  cudaFree(dT);
-  cudaFree(dq);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(flux, dq + 10 * n, (size_t)5 * n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dT, st);
+  if (dq) cudaFreeAsync(dq, st);
+  const cudaError_t es = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = es;
   if (e != cudaSuccess) return fail(h, GRHD2_ERR_CUDA, "face-flux kernel: %s", cudaGetErrorString(e));
   return GRHD2_OK;
 }
@@ -1351,8 +1384,12 @@ constexpr size_t NA_ALPHA = 0, NA_BETA = NA_ALPHA + NA_MAX, NA_GAMMA = NA_BETA +
                  NA_SQG = NA_GAMMA + 9 * NA_MAX, NA_TABLE = NA_SQG + NA_MAX, NA_QL = NA_TABLE + NFF * NA_MAX,
                  NA_QR = NA_QL + 5 * NA_MAX, NA_FLUX = NA_QR + 5 * NA_MAX, NA_TOTAL = NA_FLUX + 5 * NA_MAX;
 static_assert(NA_TOTAL == 50 * NA_MAX, "50 doubles per face");
+// one status word after the per-face regions: nonzero when a face's frame gamma^dd differs
+// from its wavespeed gamma^dd (the consistency check of build_face_table); cleared by every
+// call before its table kernel runs
+constexpr size_t NA_STATUS = NA_TOTAL;
 
-static __device__ __align__(256) double g_noalloc_scratch[NA_TOTAL];
+static __device__ __align__(256) double g_noalloc_scratch[NA_TOTAL + 1];
 
 constexpr int NA_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
@@ -1360,7 +1397,8 @@ double *g_noalloc_ptr[NA_MAX_DEVICES] = {};
 
 // per-face table of n faces (the fields build_face_table writes), built on the device
 __global__ void k_face_table(int n, int dir, const double *__restrict__ alpha, const double *__restrict__ beta,
-                             const double *__restrict__ gamma, const double *__restrict__ sqg, double *__restrict__ T) {
+                             const double *__restrict__ gamma, const double *__restrict__ sqg, double *__restrict__ T,
+                             unsigned long long *status) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= n) return;
   double g[9];
@@ -1372,11 +1410,13 @@ __global__ void k_face_table(int n, int dir, const double *__restrict__ alpha, c
   T[FF_G11 * m + f] = g[0]; T[FF_G12 * m + f] = g[3]; T[FF_G13 * m + f] = g[6];
   T[FF_G22 * m + f] = g[4]; T[FF_G23 * m + f] = g[7]; T[FF_G33 * m + f] = g[8];
   T[FF_SQG * m + f] = sqg[f];
-  T[FF_GUP * m + f] = gamma_up_dd(g, dir);
+  const double gup_w = gamma_up_dd(g, dir);
+  T[FF_GUP * m + f] = gup_w;
   double cof[9], gup;
   const bool ok = face_frame(g, dir, cof, &gup);
 #pragma unroll
   for (int q = 0; q < 9; ++q) T[(FF_COF + q) * m + f] = cof[q];
+  if (ok && __double_as_longlong(gup) != __double_as_longlong(gup_w)) atomicOr(status, 1ull);
   T[FF_FRAME_OK * m + f] = ok ? 1.0 : 0.0;
   T[FF_ZERO * m + f] = 0.0;
 }
@@ -1426,8 +1466,10 @@ int grhd2_gpu_riemann_faces_noalloc(grhd2_gpu *h, int n, int dir, const double *
   CUDA_TRY(h, cudaMemcpyAsync(s + NA_SQG, sqg, m * sizeof(double), cudaMemcpyHostToDevice, st));
   CUDA_TRY(h, cudaMemcpyAsync(s + NA_QL, qL, 5 * m * sizeof(double), cudaMemcpyHostToDevice, st));
   CUDA_TRY(h, cudaMemcpyAsync(s + NA_QR, qR, 5 * m * sizeof(double), cudaMemcpyHostToDevice, st));
+  unsigned long long *status = (unsigned long long *)(s + NA_STATUS);
+  CUDA_TRY(h, cudaMemsetAsync(status, 0, sizeof *status, st));
   k_face_table<<<nblocks(n, 128), 128, 0, st>>>(n, dir, s + NA_ALPHA, s + NA_BETA, s + NA_GAMMA, s + NA_SQG,
-                                                s + NA_TABLE);
+                                                s + NA_TABLE, status);
   if (int rc = launch_check(h)) return rc;
   if (h->mixed)
     k_riemann_faces<float><<<nblocks(n, 128), 128, 0, st>>>(h->G.phys, n, dir, s + NA_QL, s + NA_QR, s + NA_TABLE,
@@ -1437,7 +1479,10 @@ int grhd2_gpu_riemann_faces_noalloc(grhd2_gpu *h, int n, int dir, const double *
                                                              s + NA_FLUX, 0);
   if (int rc = launch_check(h)) return rc;
   CUDA_TRY(h, cudaMemcpyAsync(flux, s + NA_FLUX, 5 * m * sizeof(double), cudaMemcpyDeviceToHost, st));
+  unsigned long long bad = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&bad, status, sizeof bad, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(h, cudaStreamSynchronize(st));
+  if (bad) return fail(h, GRHD2_ERR_ARG, "internal: frame gamma^dd differs from the wavespeed gamma^dd");
   return GRHD2_OK;
 }
 
@@ -1596,7 +1641,7 @@ int grhd2_gpu_snapshot_begin(grhd2_gpu *h, double *up_host) {
   }
   // the previous snapshot's copy must have left the buffer before it is overwritten
   if (h->snap_pending) CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->snap_done, 0));
-  k_cons_out<<<nblocks(h->G.ncell, 256), 256, 0, h->stream>>>(h->G, h->G.UP, h->snap);
+  k_cons_out<<<nblocks(h->G.ncell, LAYOUT_BS), LAYOUT_BS, 0, h->stream>>>(h->G, h->G.UP, h->snap);
   if ((rc = launch_check(h))) return rc;
   CUDA_TRY(h, cudaEventRecord(h->snap_taken, h->stream));
   CUDA_TRY(h, cudaStreamWaitEvent(h->snap_stream, h->snap_taken, 0));
@@ -1656,7 +1701,8 @@ void grhd2_gpu_destroy(grhd2_gpu *h) {
   }
   if (h->snap_taken) cudaEventDestroy(h->snap_taken);
   if (h->snap_done) cudaEventDestroy(h->snap_done);
-  void *bufs[] = {h->G.P, h->G.U, h->G.UP, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1], h->G.F[2], h->G.cnt, h->G.clock,
+  void *bufs[] = {h->G.P, h->G.Prot[0], h->G.Prot[1], h->G.U, h->G.UP, h->G.Uc, h->G.UPc, h->G.RHS, h->G.Q, h->G.F[0], h->G.F[1],
+                  h->G.F[2], h->G.cnt, h->G.clock,
                   h->centre, h->face[0], h->face[1], h->face[2], h->centre_f, h->face_f[0], h->face_f[1], h->face_f[2],
                   h->inj, h->dust, h->xc, h->frozen[0], h->frozen[1],
                   h->frozen[2], h->red, h->staging, h->diag, h->snap, h->vtk};
@@ -1721,6 +1767,8 @@ int grhd2_gpu_batch_cons_to_prim(grhd2_gpu_batch *b) {
     else k_c2p_batch<double><<<nb, CELL_BS, 0, b->stream>>>(b->d_grids, grp.d_map + grp.off[K_CELL]);
     if (int rc = blaunch_check(b, "c2p_batch")) return rc;
   }
+  for (grhd2_gpu *h : b->m)
+    if (int rc = clear_carries(h, b->stream)) return bfail(b, rc, "%s", h->err.c_str());
   for (grhd2_gpu *h : b->m) h->prims_set = true;
   return GRHD2_OK;
 }

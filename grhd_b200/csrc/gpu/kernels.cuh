@@ -187,17 +187,57 @@ __global__ void k_prims_out(const GridDev G, const PT *__restrict__ Pin, double 
 }
 
 // u(5,nx,ny,nz) AoS <-> SoA
-__global__ void k_cons_in(const GridDev G, const double *__restrict__ uf, double *__restrict__ U) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= G.ncell) return;
+// Conserved state between the reference's layout u(5, nx, ny, nz) (variable fastest: the
+// upload/download staging and the checkpoint snapshot) and the SoA planes.  Launched with
+// LAYOUT_BS threads per block, one cell each.  A block's LAYOUT_BS x 5 doubles (10 KB) are
+// contiguous and start on a 16-byte boundary (a multiple of 256 cells x 40 bytes from a
+// 16-byte aligned buffer, checked), so they move between HBM and shared memory as 128-bit
+// vectors (ld/st.global.v2.f64), while each plane is read or written one coalesced row per
+// variable.  Thread t's cell sits at s[5 t .. 5 t + 4] (stride 5 doubles: two-way bank
+// conflicts at most).
+constexpr int LAYOUT_BS = 256;
+__global__ void __launch_bounds__(LAYOUT_BS) k_cons_in(const GridDev G, const double *__restrict__ uf,
+                                                       double *__restrict__ U) {
+  __shared__ __align__(16) double s[NEQ * LAYOUT_BS];
+  const long long c0 = (long long)blockIdx.x * LAYOUT_BS;
+  const int cells = (int)min((long long)LAYOUT_BS, G.ncell - c0);
+  const int nd = cells * NEQ;
+  const double *src = uf + c0 * NEQ;
+  if (((uintptr_t)uf & 15u) == 0) {
+    const double2 *src2 = reinterpret_cast<const double2 *>(src);
+    double2 *s2 = reinterpret_cast<double2 *>(s);
+    for (int q = (int)threadIdx.x; q < nd / 2; q += LAYOUT_BS) s2[q] = __ldg(&src2[q]);
+    if ((nd & 1) && threadIdx.x == 0) s[nd - 1] = src[nd - 1];
+  } else {
+    for (int q = (int)threadIdx.x; q < nd; q += LAYOUT_BS) s[q] = src[q];
+  }
+  __syncthreads();
+  const int t = (int)threadIdx.x;
+  if (t >= cells) return;
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v) U[v * G.pplane + c] = uf[5 * c + v];
+  for (int v = 0; v < NEQ; ++v) U[v * G.pplane + c0 + t] = s[NEQ * t + v];
 }
-__global__ void k_cons_out(const GridDev G, const double *__restrict__ U, double *__restrict__ uf) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= G.ncell) return;
+__global__ void __launch_bounds__(LAYOUT_BS) k_cons_out(const GridDev G, const double *__restrict__ U,
+                                                        double *__restrict__ uf) {
+  __shared__ __align__(16) double s[NEQ * LAYOUT_BS];
+  const long long c0 = (long long)blockIdx.x * LAYOUT_BS;
+  const int cells = (int)min((long long)LAYOUT_BS, G.ncell - c0);
+  const int nd = cells * NEQ;
+  const int t = (int)threadIdx.x;
+  if (t < cells) {
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v) uf[5 * c + v] = U[v * G.pplane + c];
+    for (int v = 0; v < NEQ; ++v) s[NEQ * t + v] = U[v * G.pplane + c0 + t];
+  }
+  __syncthreads();
+  double *dst = uf + c0 * NEQ;
+  if (((uintptr_t)uf & 15u) == 0) {
+    double2 *dst2 = reinterpret_cast<double2 *>(dst);
+    const double2 *s2 = reinterpret_cast<const double2 *>(s);
+    for (int q = t; q < nd / 2; q += LAYOUT_BS) dst2[q] = s2[q];
+    if ((nd & 1) && t == 0) dst[nd - 1] = s[nd - 1];
+  } else {
+    for (int q = t; q < nd; q += LAYOUT_BS) dst[q] = s[q];
+  }
 }
 
 // independent faces with explicit states (the Riemann entry point of the C-ABI)

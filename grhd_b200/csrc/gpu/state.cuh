@@ -158,6 +158,8 @@ struct GridDev {
   void *Prot[2];                // the stage kernel's rotation buffers P2, P3 (1D and 2D grids; stage.cuh)
   FastDiv stage_ntx;            // stage-kernel tiles along i
   double *U, *UP, *RHS;         // conserved u, up; RHS scratch of grhd2_gpu_calc_rhs
+  void *Uc, *UPc;               // carries of the compensated accumulation (u + Uc, up + UPc)
+  int carry;                    // 0: none, 1: FP64 carries, 2: FP32 carries
   void *F[3];                   // face fluxes per direction
   void *Q;                      // interface states of the direction being processed
   unsigned long long *cnt;      // failure / floor counters

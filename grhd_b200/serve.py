@@ -143,7 +143,8 @@ class GpuEngine:
 
     def bytes_needed(self, req: Request) -> int:
         from . import native as N
-        cfg = self.problem(req).config(0 if self.precision == "fp64" else 1)
+        from .solver import PRECISION
+        cfg = self.problem(req).config(PRECISION[self.precision])
         return int(N.gpu_lib().grhd2_gpu_device_bytes(cfg)) + 64 * 1024  # + batch descriptors
 
     def prepare(self, req: Request):

@@ -17,7 +17,11 @@ import numpy as np
 from . import native as N
 from .problem import Problem
 
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "mixed_comp64": 2, "mixed_comp32": 3}
+"""Precision policies (include/grhd2_gpu.h GRHD2_PREC_*): the FP64 parity path; the mixed
+policy (FP32 reconstruction, Riemann fluxes and metric contraction, FP64 lapse and
+sqrt(gamma) factors, con2prim and RK state); the mixed policy with the RK3 accumulation
+compensated by an FP64 or an FP32 carry."""
 
 
 class GpuError(RuntimeError):

@@ -48,7 +48,13 @@ enum { GRHD2_METRIC_MINKOWSKI = 0, GRHD2_METRIC_EF = 1, GRHD2_METRIC_KS = 2 };
 enum { GRHD2_GEOM_CARTESIAN = 0, GRHD2_GEOM_CYLINDRICAL = 1, GRHD2_GEOM_SPHERICAL = 2,
        GRHD2_GEOM_SPHEROIDAL = 3 };
 /* precision policies */
-enum { GRHD2_PREC_FP64 = 0, GRHD2_PREC_MIXED = 1 };
+/* Precision policies.  FP64: every operation in FP64 (the parity path).  MIXED: the
+ * reconstruction, Riemann fluxes and the metric contraction of the sources in FP32, their
+ * lapse and sqrt(gamma) factors, con2prim and the RK state u, up in FP64.  MIXED_COMP64 and
+ * MIXED_COMP32: MIXED with the RK3 accumulation compensated -- up and u carry the rounding
+ * error of every stage combination in a second array (a double-double state: up + carry),
+ * the carry stored in FP64 or in FP32. */
+enum { GRHD2_PREC_FP64 = 0, GRHD2_PREC_MIXED = 1, GRHD2_PREC_MIXED_COMP64 = 2, GRHD2_PREC_MIXED_COMP32 = 3 };
 
 /* Filled by the Fortran side from the globals of variables.f90.  case_id selects the
  * boundary routine of conditions.f90:773 (1 Sod, 2 strong shock, 3 Shu-Osher, 4 KHI,
@@ -196,16 +202,21 @@ int grhd2_gpu_riemann_faces(grhd2_gpu *h, int n, int dir, const double *qL, cons
                             const double *sqg, double *flux);
 /* Allocation-free variant of grhd2_gpu_riemann_faces (no counterpart in the reference):
  * same arguments, same results, but it never allocates memory, on the device or the host.
- * grhd2_gpu_riemann_faces allocates device buffers on every call; a caller that runs
- * under a fixed memory budget (the device memory is already handed out to a caching
- * allocator or to resident grids), or that must not stall other streams (cudaMalloc and
- * cudaFree can synchronise the whole device), can use this one instead.
+ * grhd2_gpu_riemann_faces allocates device buffers on every call (from the device's
+ * stream-ordered pool); a caller that runs under a fixed memory budget (the device memory
+ * is already handed out to a caching allocator or to resident grids), or whose process
+ * may not allocate device memory at all, can use this one instead.
  *  - Scratch is one fixed device array in the library, GRHD2_GPU_NOALLOC_MAX_FACES faces
  *    of 50 doubles each (6.6 MB).  n > GRHD2_GPU_NOALLOC_MAX_FACES returns GRHD2_ERR_ARG.
  *  - Nothing in the scratch has to start at zero: each call writes every element it
- *    later reads.
+ *    later reads, and clears the one status word it checks (a face whose frame gamma^dd
+ *    differs from its wavespeed gamma^dd returns GRHD2_ERR_ARG, as in
+ *    grhd2_gpu_riemann_faces).
  *  - The first call on a device looks up the scratch address (cudaGetSymbolAddress) and
- *    caches it; make that first call before any stream capture.
+ *    caches it; make that first call before any stream capture.  The cached address
+ *    belongs to the device's context at that time: after cudaDeviceReset (or a reset of
+ *    the primary context by another library in the process) it is stale, and the process
+ *    must not call this entry point on that device again.
  *  - The scratch is shared by every handle of a device: calls made at the same time from
  *    several host threads on the same device race on it.  Serialise them.
  * The call copies and launches on the handle's stream and returns after the flux is on
