@@ -37,7 +37,7 @@ __device__ __forceinline__ void sources(const Phys &P, const Col &col, const dou
   if (P.srhd) return;
   auto ld = [&](int fld) { return R(col(fld)); };
   constexpr bool mixed = sizeof(R) == sizeof(float);
-  R src[NEQ];
+  R src[NEQ] = {R(0), R(0), R(0), R(0), R(0)};  // D has no source
   const R alpha = ld(CF_ALPHA), sqg = ld(CF_SQG);
   FaceMetric<R> m;
   m.g11 = ld(CF_G11); m.g12 = ld(CF_G12); m.g13 = ld(CF_G13); m.g22 = ld(CF_G22); m.g23 = ld(CF_G23); m.g33 = ld(CF_G33);
