@@ -14,8 +14,9 @@ Two measurements, each printed as one JSON line:
          (time loop only, after one warm-up step)
          python -m oracle.stopwatch run --problem fishbone_equatorial --keys '{...}' --seconds 15
   serve  a sample of the serving stream as concurrent single-thread processes, one per
-         physical core, each taking the next arrived request (the campaign script's
-         slots): p50/p99 time to solution and aggregate zone-updates/s
+         physical core and pinned to it (the campaign script's slots, each under its own
+         taskset), each taking the next arrived request: p50/p99 time to solution and
+         aggregate zone-updates/s
          python -m oracle.stopwatch serve --requests 256 --michel-final-time 2
 
 Both run in a process of their own, so the OpenMP settings are in place before the
@@ -58,9 +59,9 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE, "stopwatch"], check=True)
 
 
-def _omp_env(threads: int) -> None:
+def _omp_env(threads: int, bind: str = "close") -> None:
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    os.environ["OMP_PROC_BIND"] = "close"
+    os.environ["OMP_PROC_BIND"] = bind
     os.environ["OMP_DYNAMIC"] = "false"
 
 
@@ -89,6 +90,16 @@ def time_run(problem: str, keys: dict, seconds: float, steps: int | None) -> dic
 
 
 # ---- serving sample -----------------------------------------------------------------
+def _pin(counter, cpus):
+    """Pool initializer: this worker runs on one CPU of its own (the campaign script runs
+    each slot under `taskset -c`).  OpenMP binding stays off: with one thread per process
+    and OMP_PROC_BIND set, every process would bind its thread to the same first place."""
+    with counter.get_lock():
+        k = counter.value
+        counter.value += 1
+    os.sched_setaffinity(0, {cpus[k % len(cpus)]})
+
+
 def _solve(job):
     """One request on one thread: host set-up, then the reference time loop to its final
     time (what one single-thread reference process does for one .par file)."""
@@ -108,7 +119,9 @@ def time_serve(nreq: int, seed: int, rate: float, michel_final_time: float, work
     from grhd_b200.serve import make_stream
     reqs = make_stream(nreq, seed=seed, rate=rate, michel_final_time=michel_final_time)
     ctx = mp.get_context("spawn")
-    with ctx.Pool(workers) as pool:
+    cpus = sorted(os.sched_getaffinity(0))
+    counter = ctx.Value("i", 0)
+    with ctx.Pool(workers, initializer=_pin, initargs=(counter, cpus)) as pool:
         pool.map(int, range(workers))  # start the workers before the clock
         t0 = time.time()
         pending = []
@@ -125,6 +138,7 @@ def time_serve(nreq: int, seed: int, rate: float, michel_final_time: float, work
     return {"requests": nreq, "zone_updates": int(zu), "makespan_s": span, "zone_updates_per_s": zu / span,
             "tts_p50_s": float(np.percentile(tts, 50)), "tts_p99_s": float(np.percentile(tts, 99)),
             "tts_mean_s": float(tts.mean()), "processes": workers, "threads_per_process": 1,
+            "pinning": "one CPU per process (sched_setaffinity)",
             "sample": f"{nreq} requests of the stream (seed {seed}), {rate:g} arrivals/s, "
                       f"Michel final time {michel_final_time:g} M"}
 
@@ -155,7 +169,7 @@ def main(argv=None):
         _omp_env(threads)
         out = time_run(args.problem, json.loads(args.keys), args.seconds, args.steps)
     else:
-        _omp_env(1)
+        _omp_env(1, bind="false")
         out = time_serve(args.requests, args.seed, args.rate, args.michel_final_time,
                          args.processes or host["physical_cores"])
     out.update(host=host, flags=FLAGS, omp={k: os.environ[k] for k in ("OMP_NUM_THREADS", "OMP_PROC_BIND",

@@ -199,25 +199,38 @@ def test_cfl_matches_oracle():
         assert g.cfl() == o.cfl()
 
 
-@pytest.mark.parametrize("maker,kw,steps", [
-    (torus_2p5d, dict(nx=128, nz=64), 60),
-    (torus_3d, dict(nx=32, ny=16, nz=16), 10),
-    (michel, dict(nx=512), 200),
-    (shock_tube, dict(nx=400), 200),
+# Relative L1 per conserved variable (D, tau, S_1, S_2, S_3), each in its own norm, that
+# the mixed policies must meet against the FP64 oracle after the steps of each case.  The
+# stated bar is 1e-5 on the 2.5D torus.  Measured (all three mixed policies agree to three
+# digits): 2.5D torus 2.0e-8 .. 3.7e-8; 3D torus 2.0e-6 .. 3.2e-6 and, for S_theta, 6.2e-4
+# -- S_theta is ~0 by symmetry, so its own norm is tiny and its relative error large (its
+# absolute error is that of the other momenta); Michel 2.9e-7 .. 3.7e-7; shock tube
+# 2.2e-7 .. 9.8e-7.
+MIXED_L1_BOUND = {
+    "torus_2p5d": [1e-5] * 5,
+    "torus_3d": [1e-5, 1e-5, 1e-5, 2e-3, 1e-5],
+    "michel": [1e-5] * 5,
+    "shock_tube": [1e-5] * 5,
+}
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_comp64", "mixed_comp32"])
+@pytest.mark.parametrize("name,maker,kw,steps", [
+    ("torus_2p5d", torus_2p5d, dict(nx=128, nz=64), 60),
+    ("torus_3d", torus_3d, dict(nx=32, ny=16, nz=16), 10),
+    ("michel", michel, dict(nx=512), 200),
+    ("shock_tube", shock_tube, dict(nx=400), 200),
 ])
-def test_mixed_policy_l1(maker, kw, steps):
-    """Mixed policy (FP32 reconstruction, Riemann fluxes and sources; FP64 con2prim with the
-    seeded root finder and FP64 RK state) against the FP64 oracle after the same steps:
-    relative L1 per conserved variable at most 1e-5, the bar stated for the 2.5D torus."""
+def test_mixed_policy_l1(name, maker, kw, steps, precision):
+    """Mixed policies (FP32 reconstruction, Riemann fluxes and metric contraction; FP64
+    lapse and sqrt(gamma) factors, con2prim with the seeded root finder and RK state, the
+    RK accumulation plain or compensated with an FP64 or FP32 carry) against the FP64
+    oracle after the same steps: relative L1 per conserved variable, each in its own norm,
+    within MIXED_L1_BOUND."""
     pb = maker(**kw)
-    o, g, up, p = run_pair(pb, nsteps=steps, precision="mixed")
+    o, g, up, p = run_pair(pb, nsteps=steps, precision=precision)
     l1 = rel_l1(up, o.up)
-    if maker is torus_3d:
-        # S_theta of the torus is nearly zero by symmetry: its error is measured against the
-        # magnitude of the whole momentum (sum of |S_i| over cells and components)
-        a, b = up.reshape(-1, 5), o.up.reshape(-1, 5)
-        l1[3] = np.abs(a[:, 3] - b[:, 3]).sum() / np.abs(b[:, 2:5]).sum()
-    assert np.all(l1 <= 1e-5), f"mixed relative L1 per variable {l1}"
+    assert np.all(l1 <= np.array(MIXED_L1_BOUND[name])), f"{precision} relative L1 per variable {l1}"
 
 
 def test_async_upload_download_match_sync():
@@ -245,3 +258,34 @@ def test_async_upload_download_match_sync():
     assert np.array_equal(up_b, up_sync) and np.array_equal(p_b, p_sync)
     g.close()
     h.close()
+
+
+@pytest.mark.parametrize("precision", ["mixed_comp64", "mixed_comp32"])
+def test_compensated_accumulation_carries(precision):
+    """The compensated policies keep a carry beside u and up: after the same steps their
+    state differs from the plain mixed policy's in the last bits (the rounding the FP64
+    combination drops is carried, not lost), and the carries restart at zero when up is
+    uploaded -- a grid that re-uploads its own downloaded state continues exactly as a
+    fresh grid started from that state."""
+    pb = torus_2p5d(nx=64, nz=32)
+    p0 = initial_state(pb)
+    runs = {}
+    for prec in ("mixed", precision):
+        g = GpuGrid(pb, precision=prec, upload_initial=False)
+        g.upload(p=p0)
+        g.prim_to_cons()
+        g.run(0.0, 1e30, 20)
+        runs[prec] = g
+    up_m, _ = runs["mixed"].download(want_p=False)
+    up_c, p_c = runs[precision].download(p_template=p0)
+    assert not np.array_equal(up_m, up_c), "the carries change nothing"
+    assert np.all(rel_l1(up_c, up_m) <= 1e-12)
+    a = runs[precision]
+    a.upload(up=up_c, p=p_c)  # the carries restart at zero
+    a.run(0.0, 1e30, 7)
+    b = GpuGrid(pb, precision=precision, upload_initial=False)
+    b.upload(up=up_c, p=p_c)
+    b.run(0.0, 1e30, 7)
+    assert np.array_equal(a.download(want_p=False)[0], b.download(want_p=False)[0])
+    for g in (*runs.values(), b):
+        g.close()
