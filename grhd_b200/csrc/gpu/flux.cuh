@@ -429,9 +429,15 @@ __device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned
 // Resident 128-thread blocks per SM for the fused kernel.  FP32 (mixed policy): 10 with
 // HLLE (48 registers; 8 and 12 measured 2.5 % and 0-1 % slower on the batched 2.5D torus),
 // 8 with HLLC, whose larger state spills at 48 (64 registers; 3D torus +2.8 %, its x faces
-// -8 %).  The FP64 instantiation keeps its registers.
+// -8 %).  FP64: 8 with HLLE (64 registers, a few spills; 32 tori 400x1x200: 7.90e8
+// zone-updates/s against 7.36e8 for the split kernels and 6.61e8 with the 104 registers it
+// takes unbounded; 6 and 10 blocks 7.47e8 and 7.87e8), 4 with HLLC (3D torus 4.05e8, 2 and
+// 6-8 blocks slower -- the split kernels, 4.89e8, stay ahead there and the autotuner keeps
+// them).
 template <int RS, class R>
-constexpr int flux_min_blocks() { return sizeof(R) == sizeof(float) ? (RS == RS_HLLC ? 8 : 10) : 1; }
+constexpr int flux_min_blocks() {
+  return sizeof(R) == sizeof(float) ? (RS == RS_HLLC ? 8 : 10) : (RS == RS_HLLC ? 4 : 8);
+}
 template <int DIR, int REC, int RS, class R, class PT>
 __global__ void __launch_bounds__(FLUX_BS, flux_min_blocks<RS, R>())
     k_flux(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map) {
