@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256, RECON_MIN_BLOCKS) k_recon(const GridDev *
   R ew[NEQ][6];  // an edge face's window, boundary-filled (local memory)
   if (!inside) edge_window<DIR>(Pin, G, x, lo, hi, ew);
   auto ld = [&](int w, int m) -> R {
-    return inside ? R((double)GRHD_LDP(&Pin[w * G.pplane + base + m * stride])) : ew[w][m];
+    return inside ? R(GRHD_LDP(&Pin[w * G.pplane + base + m * stride])) : ew[w][m];
   };
   int br = BR_GODUNOV;
   if (REC != REC_GODUNOV) {
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(256, RECON_MIN_BLOCKS) k_recon(const GridDev *
     if (inside) {
       const PT *row = Pin + (base + (long long)v * pplane);
 #pragma unroll
-      for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? R((double)GRHD_LDP(row + m * ustride)) : R(0);
+      for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? R(GRHD_LDP(row + m * ustride)) : R(0);
     } else {
 #pragma unroll
       for (int m = 0; m < 6; ++m) s[m] = (m >= lo && m <= hi) ? ew[v][m] : R(0);
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(256, 5) k_recon_var(const GridDev *__restrict_
   const long long pplane = G.pplane;
   const unsigned ustride = (unsigned)stride;
   auto ld = [&](int w, int m) -> R {
-    return inside ? R((double)GRHD_LDP(Pin + (base + (long long)w * pplane) + m * ustride))
+    return inside ? R(GRHD_LDP(Pin + (base + (long long)w * pplane) + m * ustride))
                   : R(load_var<DIR>(Pin, G, x, x.face - 2 + m, w));
   };
   R s[6];
@@ -360,7 +360,7 @@ __device__ __forceinline__ void flux_item(const GridDev &G, unsigned a, unsigned
     if (inside) {
       const PT *row = Pin + (base + (long long)w * pplane);
 #pragma unroll
-      for (int m = 0; m < 6; ++m) out[m] = (m >= a && m <= b) ? R((double)GRHD_LDP(row + m * ustride)) : R(0);
+      for (int m = 0; m < 6; ++m) out[m] = (m >= a && m <= b) ? R(GRHD_LDP(row + m * ustride)) : R(0);
     } else {
 #pragma unroll
       for (int m = 0; m < 6; ++m) out[m] = (m >= a && m <= b) ? ew[w][m] : R(0);
