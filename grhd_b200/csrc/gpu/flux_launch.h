@@ -101,6 +101,25 @@ extern template cudaError_t run_persistent<double, double>(int, int, bool, int *
 extern template cudaError_t run_persistent<float, float>(int, int, bool, int *, const PersistentArgs &, int, int,
                                                          cudaStream_t);
 
+// persistent stage kernel (persistent.cuh): whole steps of a group of 1D grids in one
+// cooperative launch over the stage kernel's tiles (the group's K_STAGE block map)
+struct PersistentStageArgs {
+  const GridDev *grids;
+  const BlockMap *tiles;
+  int ntiles;
+  const int *members;
+  int nmembers;
+  unsigned *bar;
+  unsigned *status;
+};
+template <class R, class PT>
+cudaError_t run_persistent_stage(int rec, int rs, bool query, int *max_blocks, const PersistentStageArgs &a,
+                                 int nsteps, int nblocks, cudaStream_t s);
+extern template cudaError_t run_persistent_stage<double, double>(int, int, bool, int *, const PersistentStageArgs &,
+                                                                 int, int, cudaStream_t);
+extern template cudaError_t run_persistent_stage<float, float>(int, int, bool, int *, const PersistentStageArgs &,
+                                                               int, int, cudaStream_t);
+
 // fused face fluxes of direction dir (recon + Riemann in one kernel)
 template <class R, class PT>
 inline void launch_flux(int dir, int rec, int rs, const GridDev *grids, const BlockMap *map, int nblocks,

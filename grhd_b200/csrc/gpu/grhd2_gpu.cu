@@ -180,6 +180,7 @@ struct Group {
   int nseg_face = 0, nseg_cell = 0;
   long long n_face = 0, n_cell = 0;
   int max_blocks = 0;  // resident blocks of the group's persistent instantiation
+  int max_blocks_stage = 0;  // resident blocks of its persistent stage kernel (stage groups of 1D grids)
   int cell_dirs = 1;   // the most active directions of a member grid (cell kernel staging)
   bool stage = false;  // steps run the stage kernel (one launch per stage) instead of face and cell kernels
 };
@@ -491,6 +492,12 @@ int build_batch(grhd2_gpu_batch *b) {
     cudaError_t e = grp.mixed ? run_persistent<float, float>(grp.rec, grp.rs, true, &grp.max_blocks, {}, 0, 0, b->stream)
                               : run_persistent<double, double>(grp.rec, grp.rs, true, &grp.max_blocks, {}, 0, 0, b->stream);
     if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "persistent kernel occupancy: %s", cudaGetErrorString(e));
+    if (grp.stage && grp.sd == 0) {
+      e = grp.mixed ? run_persistent_stage<float, float>(grp.rec, grp.rs, true, &grp.max_blocks_stage, {}, 0, 0, b->stream)
+                    : run_persistent_stage<double, double>(grp.rec, grp.rs, true, &grp.max_blocks_stage, {}, 0, 0,
+                                                           b->stream);
+      if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "persistent stage kernel occupancy: %s", cudaGetErrorString(e));
+    }
   }
   BCUDA_TRY(b, cudaMallocAsync((void **)&b->d_bar, 4 * sizeof(unsigned), b->stream));
   BCUDA_TRY(b, cudaMemsetAsync(b->d_bar, 0, 4 * sizeof(unsigned), b->stream));
@@ -498,7 +505,8 @@ int build_batch(grhd2_gpu_batch *b) {
   b->persistent = b->step_request == GRHD2_STEP_PERSISTENT;
   if (b->persistent)
     for (const auto &grp : b->groups)
-      if (grp.max_blocks <= 0) return bfail(b, GRHD2_ERR_CUDA, "the persistent step kernel cannot be resident");
+      if (grp.max_blocks <= 0 || (grp.stage && grp.sd == 0 && grp.max_blocks_stage <= 0))
+        return bfail(b, GRHD2_ERR_CUDA, "the persistent step kernel cannot be resident");
   BCUDA_TRY(b, cudaStreamSynchronize(b->stream));  // host vectors go out of scope
   return 0;
 }
@@ -625,6 +633,23 @@ int enqueue_step(grhd2_gpu_batch *b, bool branches = false) {
 // persistent kernel (groups run one after the other on the batch stream)
 int enqueue_persistent(grhd2_gpu_batch *b, long long nsteps) {
   for (const auto &grp : b->groups) {
+    if (grp.stage && grp.sd == 0) {  // 1D grids: the persistent form of the stage kernel
+      if (grp.nb[K_STAGE] <= 0) continue;
+      const PersistentStageArgs a{b->d_grids, grp.d_map + grp.off[K_STAGE], grp.nb[K_STAGE], grp.d_members,
+                                  (int)grp.members.size(), b->d_bar, b->d_bar + 2};
+      const int blocks = std::max(1, std::min(grp.max_blocks_stage, grp.nb[K_STAGE]));
+      for (long long done = 0; done < nsteps;) {
+        const int chunk = (int)std::min<long long>(nsteps - done, 1 << 30);
+        BCUDA_TRY(b, cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), b->stream));  // arrivals, generation
+        cudaError_t e = grp.mixed ? run_persistent_stage<float, float>(grp.rec, grp.rs, false, nullptr, a, chunk, blocks, b->stream)
+                                  : run_persistent_stage<double, double>(grp.rec, grp.rs, false, nullptr, a, chunk, blocks,
+                                                                         b->stream);
+        if (e != cudaSuccess) return bfail(b, GRHD2_ERR_CUDA, "persistent stage kernel launch: %s", cudaGetErrorString(e));
+        if (int rc = blaunch_check(b, "persistent_stage")) return rc;
+        done += chunk;
+      }
+      continue;
+    }
     const PersistentArgs a{b->d_grids, grp.d_members, (int)grp.members.size(), grp.d_seg, grp.nseg_face, grp.n_face,
                            grp.d_seg + grp.nseg_face, grp.nseg_cell, grp.n_cell, b->d_bar, b->d_bar + 2};
     const long long need = std::max(std::max(grp.n_face, grp.n_cell), (long long)grp.members.size());

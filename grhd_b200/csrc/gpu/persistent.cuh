@@ -21,6 +21,7 @@
 #include "cell.cuh"
 #include "flux.cuh"
 #include "flux_launch.h"
+#include "stage.cuh"
 
 namespace grhd {
 
@@ -110,6 +111,74 @@ __global__ void __launch_bounds__(FLUX_BS)
       advance_clock(grids[members[it]].clock);
     if (!grid_barrier(bar, nblk, status)) return;
   }
+}
+
+// Whole steps of a group of 1D grids in one cooperative launch, built on the stage kernel
+// (stage.cuh): each stage is one pass of the group's tiles (the stage kernel's block map,
+// ntiles entries) spread over the resident blocks, then one grid barrier; after the third
+// stage every grid's clock advances, then a barrier.  Four barriers per step, against seven
+// for k_persistent, and the stage kernel's tile work (faces and cells through shared
+// memory).  The primitives rotate through P, P2, P3 as in the stage kernel, so a stage
+// never reads what it writes; what another block wrote in an earlier stage is read through
+// L2 (GRHD_LDP, -dlcm=cg in this translation unit).
+template <int REC, int RS, class R, class PT>
+__global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
+    k_persistent_stage(const GridDev *__restrict__ grids, const BlockMap *__restrict__ tiles, int ntiles,
+                       const int *__restrict__ members, int nmembers, int nsteps, unsigned *bar, unsigned *status) {
+  extern __shared__ __align__(16) unsigned char stage_smem[];
+  const unsigned nblk = gridDim.x;
+  for (int step = 0; step < nsteps; ++step) {
+    for (int mode = 1; mode <= 3; ++mode) {
+      for (int t = (int)blockIdx.x; t < ntiles; t += (int)nblk) {
+        __syncthreads();  // the previous tile's cell phase is done with shared memory
+        stage_tile<0, REC, RS, R, PT>(grids, tiles[t], mode, stage_smem);
+      }
+      if (!grid_barrier(bar, nblk, status)) return;
+    }
+    for (int it = (int)(blockIdx.x * STAGE_BS + threadIdx.x); it < nmembers; it += (int)(nblk * STAGE_BS))
+      advance_clock(grids[members[it]].clock);
+    if (!grid_barrier(bar, nblk, status)) return;
+  }
+}
+
+template <int REC, int RS, class R, class PT>
+inline cudaError_t persistent_stage_rs(bool query, int *max_blocks, const PersistentStageArgs &a, int nsteps,
+                                       int nblocks, cudaStream_t s) {
+  auto kern = k_persistent_stage<REC, RS, R, PT>;
+  const size_t smem = stage_smem_bytes<0, R>();
+  if (query) {
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, STAGE_BS, smem);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    *max_blocks = per_sm * sms;
+    return cudaSuccess;
+  }
+  const GridDev *g = a.grids;
+  const BlockMap *tl = a.tiles;
+  int nt = a.ntiles;
+  const int *m = a.members;
+  int nm = a.nmembers;
+  unsigned *bar = a.bar, *st = a.status;
+  void *args[] = {&g, &tl, &nt, &m, &nm, &nsteps, &bar, &st};
+  return cudaLaunchCooperativeKernel((const void *)kern, dim3((unsigned)nblocks), dim3(STAGE_BS), args, smem, s);
+}
+
+template <class R, class PT>
+cudaError_t run_persistent_stage(int rec, int rs, bool query, int *max_blocks, const PersistentStageArgs &a,
+                                 int nsteps, int nblocks, cudaStream_t s) {
+#define GRHD_PERSIST_REC(RC)                                                                                \
+  return rs == RS_HLLC ? persistent_stage_rs<RC, RS_HLLC, R, PT>(query, max_blocks, a, nsteps, nblocks, s) \
+                       : persistent_stage_rs<RC, RS_HLLE, R, PT>(query, max_blocks, a, nsteps, nblocks, s)
+  switch (rec) {
+    case REC_GODUNOV: GRHD_PERSIST_REC(REC_GODUNOV);
+    case REC_TVD: GRHD_PERSIST_REC(REC_TVD);
+    case REC_WENO3: GRHD_PERSIST_REC(REC_WENO3);
+    case REC_MP5: GRHD_PERSIST_REC(REC_MP5);
+    default: GRHD_PERSIST_REC(REC_WENO5);
+  }
+#undef GRHD_PERSIST_REC
 }
 
 // Host side: maximum resident blocks of the instantiation for (rec, rs), and the launch.

@@ -6,4 +6,6 @@
 
 namespace grhd {
 template cudaError_t run_persistent<float, float>(int, int, bool, int *, const PersistentArgs &, int, int, cudaStream_t);
+template cudaError_t run_persistent_stage<float, float>(int, int, bool, int *, const PersistentStageArgs &, int, int,
+                                                   cudaStream_t);
 }  // namespace grhd

@@ -6,4 +6,6 @@
 
 namespace grhd {
 template cudaError_t run_persistent<double, double>(int, int, bool, int *, const PersistentArgs &, int, int, cudaStream_t);
+template cudaError_t run_persistent_stage<double, double>(int, int, bool, int *, const PersistentStageArgs &, int, int,
+                                                   cudaStream_t);
 }  // namespace grhd

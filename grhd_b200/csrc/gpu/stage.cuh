@@ -174,23 +174,22 @@ __device__ __forceinline__ void stage_buffers(const GridDev &G, int mode, const 
   pout = (PT *)(mode == 3 ? G.P : G.Prot[mode - 1]);
 }
 
-// Batched: block b works on grid map[b].grid, tile map[b].first / STAGE_BS (tiles numbered
-// with i fastest).  mode: the RK stage, 1..3.  The block's first STAGE_CELLS threads
-// update the tile's cells.
+// The work of one block on one tile, bm: grid bm.grid, tile bm.first / STAGE_BS (tiles
+// numbered with i fastest); mode: the RK stage, 1..3.  The block's first STAGE_CELLS
+// threads update the tile's cells.  k_stage runs one tile per block; the persistent stage
+// kernel (persistent.cuh) loops over tiles.
 template <int SD, int REC, int RS, class R, class PT>
-__global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
-    k_stage(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map, int mode) {
+__device__ __forceinline__ void stage_tile(const GridDev *__restrict__ grids, const BlockMap bm, int mode,
+                                           unsigned char *stage_smem) {
   using Gm = StageGeom<SD>;
   constexpr int TX = Gm::TX, TR = Gm::TR, BX = Gm::BX, NBOX = Gm::NBOX, NFX = Gm::NFX, NFR = Gm::NFR;
   constexpr bool SLICE = Gm::SLICE;
   constexpr int RD = SD == 0 ? 1 : SD;  // the second direction (1D: none)
-  extern __shared__ __align__(16) unsigned char stage_smem[];
   R *s_p = (R *)stage_smem;
   R *s_fx = (R *)(stage_smem + stage_align((size_t)NEQ * NBOX * sizeof(R)));
   R *s_fr = (R *)((unsigned char *)s_fx + stage_align((size_t)NEQ * NFX * sizeof(R)));
   R *slice = (R *)((unsigned char *)s_fr + stage_align((size_t)NEQ * NFR * sizeof(R)));
 
-  const BlockMap bm = map[blockIdx.x];
   const GridDev &G = grids[bm.grid];
   const GridClock ck = *G.clock;
   if (clock_skip(ck)) return;  // the same for the whole block (one grid)
@@ -225,7 +224,7 @@ __global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
       if (i >= 1 && i <= nx && r >= 1 && r <= nr) {
         const unsigned c = cell_index(G, i, j, k);
 #pragma unroll
-        for (int v = 0; v < NEQ; ++v) q[v] = (double)__ldg(&Pin[v * G.pplane + c]);
+        for (int v = 0; v < NEQ; ++v) q[v] = (double)GRHD_LDP(&Pin[v * G.pplane + c]);
       } else if (i < 1 || i > nx) {
         load_cell<1>(Pin, G, i, j, k, q);
       } else {
@@ -305,6 +304,14 @@ __global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
       cell_core<R, PT>(G, ia, jb, x, mode, dt, in, Pout);
     }
   }
+}
+
+// Batched: block b works on tile map[b] of the launch.
+template <int SD, int REC, int RS, class R, class PT>
+__global__ void __launch_bounds__(STAGE_BS, stage_min_blocks<R>())
+    k_stage(const GridDev *__restrict__ grids, const BlockMap *__restrict__ map, int mode) {
+  extern __shared__ __align__(16) unsigned char stage_smem[];
+  stage_tile<SD, REC, RS, R, PT>(grids, map[blockIdx.x], mode, stage_smem);
 }
 
 }  // namespace grhd

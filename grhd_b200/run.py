@@ -134,6 +134,8 @@ def main(argv=None):
     ap.add_argument("--tile", type=int, default=0, help="face-kernel tile extent along i (0: automatic)")
     ap.add_argument("--stage", choices=["auto", "on", "off"], default="auto",
                     help="the stage kernel for 1D and 2D grids (one kernel per RK stage)")
+    ap.add_argument("--step-mode", choices=["auto", "graph", "persistent"], default="auto",
+                    help="stage kernels replayed as a graph, or whole steps in one persistent launch")
     ap.add_argument("--accuracy", action="store_true",
                     help="run the problem in FP64 and mixed from the same state to --final-time (or --steps) "
                          "and report the mixed-vs-FP64 L1 (and the Michel L1 against the analytic profile)")
@@ -182,6 +184,7 @@ def main(argv=None):
         batch.set_flux_variant(args.flux)
         batch.set_tile(args.tile)
     batch.set_stage_kernel(args.stage)
+    batch.set_step_mode(args.step_mode)
     batch.step(args.warmup, graph=args.graph)
     g.synchronize()
     t0 = time.perf_counter()
