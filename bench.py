@@ -15,8 +15,9 @@ Multi-GPU: one process per GPU (torchrun), each rank advances its own batch
 whole-job zone-updates/s, timed on the device as the max over ranks.
 
 ``--impl reference`` times the reference's CPU implementation of the path on the host
-cores instead: the reference (Fortran) cannot be compiled in this image (no gfortran),
-so its restatement in oracle/ is timed, with all host threads.
+cores instead: the reference (Fortran) cannot be compiled here or on the GPU hosts (no
+Fortran compiler), so its restatement in oracle/ is timed, built on the timing host with
+the reference's own optimisation flags and run on all physical cores (oracle/stopwatch.py).
 """
 from __future__ import annotations
 
@@ -380,6 +381,7 @@ def run_ours(args):
     }
     if args.serve_requests > 0:
         out["serve"] = run_serve(args)
+        out["serve_mixed"] = run_serve(args, "mixed")
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(max_seconds=args.cpu_seconds)
     if world > 1:
@@ -389,22 +391,28 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
 
 
-def run_serve(args):
+def run_serve(args, precision="fp64"):
     """A bounded sample of the serving stream (Poisson arrivals, 70 % Riemann problems of
     128-8192 cells to t = 0.4, 30 % Michel runs of 512-4096 cells) through the
-    continuous-batching server on this GPU: time to solution p50/p99 and zone-updates/s."""
+    continuous-batching server on this GPU: time to solution p50/p99 and zone-updates/s.
+    The host's load and CPU are recorded beside it: the server's host work (grid set-up,
+    batch rebuilds) shares the host cores, and the sample's figures move with them."""
     from grhd_b200.serve import GpuEngine, SolveServer, make_stream, summarize
     reqs = make_stream(args.serve_requests, seed=20260901, rate=args.serve_rate,
                        michel_final_time=args.serve_michel_final_time)
-    eng = GpuEngine("fp64")
+    load0 = os.getloadavg()
+    eng = GpuEngine(precision)
     srv = SolveServer(eng, steps_per_round=16)
     res = srv.run(reqs)
     eng.close()
     out = summarize(res)
     out.update(peak_active=srv.peak_active, rounds=srv.rounds, batch_rebuilds=srv.rebuilds,
                host_s={k: round(v, 3) for k, v in {**srv.host_s, **eng.host_s}.items()},
+               host={"nproc": os.cpu_count(), "loadavg_1min_before": round(load0[0], 2),
+                     "loadavg_1min_after": round(os.getloadavg()[0], 2)},
                sample=f"{args.serve_requests} requests of the 4096-request stream (seed 20260901), "
-                      f"{args.serve_rate:g} arrivals/s, Michel final time {args.serve_michel_final_time:g} M, FP64",
+                      f"{args.serve_rate:g} arrivals/s, Michel final time {args.serve_michel_final_time:g} M, "
+                      f"{precision}",
                timing="wall clock from each arrival to its result on the host")
     return out
 
