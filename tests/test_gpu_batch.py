@@ -321,9 +321,7 @@ def _stage_cases_mixed():
     """The shapes of _stage_cases with states the FP32 arithmetic of the mixed policy can
     represent: the shock tubes at a 10:1 pressure ratio (Sod's states) instead of the
     1.3e7 of the blast wave, whose 1e-6 right-state pressure is below FP32 round-off of
-    the left state's energy in the fluxes; HLLE on the x-y grids, whose 5 % cell-level
-    pressure noise makes FP32 HLLC fall back to HLLE at other faces than FP64 does (a
-    contact-resolving flux swapped for a diffusive one: relative L1 ~2e-3 on both paths)."""
+    the left state's energy in the fluxes."""
     sod = dict(sod_density_left=1.0, sod_pressure_left=1.0, sod_density_right=0.125, sod_pressure_right=0.1)
     return [
         shock_tube(nx=5, **sod), shock_tube(nx=257, rec="mp5", rs="hllc", sensor=True, **sod),
@@ -331,7 +329,7 @@ def _stage_cases_mixed():
         michel(nx=333, rec="weno5", rs="hllc", sensor=True),
         torus_2p5d(nx=37, nz=11), torus_2p5d(nx=70, nz=30, rec="mp5", rs="hllc", sensor=True),
         torus_2p5d(nx=20, nz=4, rec="weno3", rs="hlle", sensor=True),
-        shock_tube_xy(nx=33, ny=9, rs="hlle", **sod),
+        shock_tube_xy(nx=33, ny=9, **sod),
         shock_tube_xy(nx=80, ny=20, rec="weno5", rs="hlle", sensor=True, **sod),
     ]
 
