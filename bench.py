@@ -401,7 +401,7 @@ def run_serve(args, precision="fp64"):
     reqs = make_stream(args.serve_requests, seed=20260901, rate=args.serve_rate,
                        michel_final_time=args.serve_michel_final_time)
     load0 = os.getloadavg()
-    eng = GpuEngine(precision)
+    eng = GpuEngine(precision, metric=args.serve_metric)
     srv = SolveServer(eng, steps_per_round=16)
     res = srv.run(reqs)
     eng.close()
@@ -412,7 +412,7 @@ def run_serve(args, precision="fp64"):
                      "loadavg_1min_after": round(os.getloadavg()[0], 2)},
                sample=f"{args.serve_requests} requests of the 4096-request stream (seed 20260901), "
                       f"{args.serve_rate:g} arrivals/s, Michel final time {args.serve_michel_final_time:g} M, "
-                      f"{precision}",
+                      f"{precision}, metric tables built on the {args.serve_metric}",
                timing="wall clock from each arrival to its result on the host")
     return out
 
@@ -465,6 +465,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=256, help="serving sample size (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-michel-final-time", type=float, default=2.0)
+    ap.add_argument("--serve-metric", choices=["host", "device"], default="host",
+                    help="where the serving sample builds each request's metric tables")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -55,10 +55,11 @@ def build_host(force=False, verbose=False) -> str:
     os.makedirs(LIB, exist_ok=True)
     out = os.path.join(LIB, "libgrhd2host.so")
     srcs = _sources("host", (".cpp",))
-    hdrs = [os.path.join(INCLUDE, "grhd2_host.h"), os.path.join(INCLUDE, "grhd2_gpu.h")]
+    hdrs = [os.path.join(INCLUDE, "grhd2_host.h"), os.path.join(INCLUDE, "grhd2_gpu.h"),
+            os.path.join(CSRC, "gpu", "metric_eval.h")]
     if force or _newer(out, srcs + hdrs):
         _run([_cxx(), "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-I" + INCLUDE,
-              "-o", out] + srcs, verbose)
+              "-I" + os.path.join(CSRC, "gpu"), "-o", out] + srcs, verbose)
     return out
 
 

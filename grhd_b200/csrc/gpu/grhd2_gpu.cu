@@ -34,6 +34,7 @@
 #include "frame.h"
 #include "diag.cuh"
 #include "kernels.cuh"
+#include "metric_build.cuh"
 
 using namespace grhd;
 
@@ -707,7 +708,7 @@ int batch_steps(grhd2_gpu_batch *b, long long nsteps, bool use_graph) {
 
 int ready(grhd2_gpu *h, bool need_state) {
   if (!h) return GRHD2_ERR_ARG;
-  if (!h->metric_set) return fail(h, GRHD2_ERR_STATE, "metric tables not set (call grhd2_gpu_set_metric first)");
+  if (!h->metric_set) return fail(h, GRHD2_ERR_STATE, "metric tables not set (call grhd2_gpu_set_metric or grhd2_gpu_set_metric_analytic first)");
   const int cs = h->cfg.case_id;
   if ((cs == 7 || cs == 8 || cs == 5) && !h->bc_set)
     return fail(h, GRHD2_ERR_STATE, "boundary data not set for case %d (call grhd2_gpu_set_bc_data)", cs);
@@ -1101,6 +1102,96 @@ int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m) {
   h->metric_set = true;
   h->dt_valid = false;
   ++h->version;
+  return GRHD2_OK;
+}
+
+// face counts of the three directions' tables (0: no table), as grhd2_gpu_set_metric sizes them
+static void face_counts(const grhd2_gpu_config &c, size_t nf[3]) {
+  nf[0] = (size_t)(c.nx + 1) * c.ny;
+  nf[1] = c.ny > 1 ? (size_t)c.nx * (c.ny + 1) : 0;
+  nf[2] = c.nz > 1 ? (size_t)c.nx * c.ny : 0;
+}
+
+int grhd2_gpu_set_metric_analytic(grhd2_gpu *h, const grhd2_gpu_metric_params *mp) {
+  if (!h || !mp) return GRHD2_ERR_ARG;
+  const grhd2_gpu_config &c = h->cfg;
+  if (c.metric_kind < GRHD2_METRIC_MINKOWSKI || c.metric_kind > GRHD2_METRIC_KS || c.geom_kind < GRHD2_GEOM_CARTESIAN ||
+      c.geom_kind > GRHD2_GEOM_SPHEROIDAL)
+    return fail(h, GRHD2_ERR_ARG, "unknown metric kind %d or geometry kind %d", c.metric_kind, c.geom_kind);
+  const bool polar = c.geom_kind == GRHD2_GEOM_SPHERICAL || c.geom_kind == GRHD2_GEOM_SPHEROIDAL;
+  if (c.use_log_r && !polar)
+    return fail(h, GRHD2_ERR_ARG, "a logarithmic radial grid requires spherical or spheroidal geometry");
+  if (!std::isfinite(mp->bh_mass) || !std::isfinite(mp->a_spin) || !std::isfinite(mp->x_min) ||
+      !std::isfinite(mp->y_min))
+    return fail(h, GRHD2_ERR_ARG, "metric parameters must be finite");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  const MetricGrid g{{c.metric_kind, c.geom_kind, c.use_log_r ? 1 : 0, c.ny, mp->bh_mass, mp->a_spin},
+                     c.nx, c.ny, mp->x_min, mp->y_min, c.dx, c.dy};
+  const size_t nij = (size_t)c.nx * c.ny;
+  size_t nf[3];
+  face_counts(c, nf);
+  int rc;
+  if (!h->centre && (rc = dalloc(h, &h->centre, (size_t)NCF * nij))) return rc;
+  for (int d = 0; d < 3; ++d)
+    if (nf[d] && !h->face[d] && (rc = dalloc(h, &h->face[d], (size_t)NFF * nf[d]))) return rc;
+  if (h->mixed) {
+    if (!h->centre_f && (rc = dalloc(h, &h->centre_f, (size_t)NCF * nij))) return rc;
+    for (int d = 0; d < 3; ++d)
+      if (nf[d] && !h->face_f[d] && (rc = dalloc(h, &h->face_f[d], (size_t)NFF * nf[d]))) return rc;
+  }
+  h->metric_set = false;  // until the new tables are complete and checked
+  cudaStream_t st = h->stream;
+  unsigned long long *status = nullptr;
+  CUDA_TRY(h, cudaMallocAsync((void **)&status, sizeof *status, st));
+  CUDA_TRY(h, cudaMemsetAsync(status, 0, sizeof *status, st));
+  k_metric_centre<<<nblocks((long long)nij, 128), 128, 0, st>>>(g, h->centre, status);
+  if ((rc = launch_check(h))) return rc;
+  for (int d = 0; d < 3; ++d) {
+    if (!nf[d]) continue;
+    k_metric_face<<<nblocks((long long)nf[d], 128), 128, 0, st>>>(g, d + 1, (int)nf[d], h->face[d], status);
+    if ((rc = launch_check(h))) return rc;
+  }
+  if (h->mixed) {
+    k_metric_to_float<<<nblocks((long long)(NCF * nij), 256), 256, 0, st>>>(h->centre, h->centre_f, NCF * nij);
+    if ((rc = launch_check(h))) return rc;
+    for (int d = 0; d < 3; ++d) {
+      if (!nf[d]) continue;
+      k_metric_to_float<<<nblocks((long long)(NFF * nf[d]), 256), 256, 0, st>>>(h->face[d], h->face_f[d],
+                                                                               NFF * nf[d]);
+      if ((rc = launch_check(h))) return rc;
+    }
+  }
+  unsigned long long bad = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&bad, status, sizeof bad, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaFreeAsync(status, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  if (bad & MB_ASYM) return fail(h, GRHD2_ERR_ARG, "device-built metric tables are not exactly symmetric");
+  if (bad & MB_FRAME) return fail(h, GRHD2_ERR_ARG, "internal: frame gamma^dd differs from the wavespeed gamma^dd");
+  h->G.centre = h->centre;
+  for (int d = 0; d < 3; ++d) h->G.face[d] = h->face[d];
+  h->G.centre_f = h->centre_f;
+  for (int d = 0; d < 3; ++d) h->G.face_f[d] = h->face_f[d];
+  h->metric_set = true;
+  h->dt_valid = false;
+  ++h->version;
+  return GRHD2_OK;
+}
+
+int grhd2_gpu_metric_table(grhd2_gpu *h, int32_t which, double *out, size_t n, size_t *n_out) {
+  if (!h) return GRHD2_ERR_ARG;
+  if (which < 0 || which > 3) return fail(h, GRHD2_ERR_ARG, "metric table %d: expected 0 (centre) or 1-3 (faces)", which);
+  if (!h->metric_set) return fail(h, GRHD2_ERR_STATE, "metric tables not set");
+  const grhd2_gpu_config &c = h->cfg;
+  size_t nf[3];
+  face_counts(c, nf);
+  const double *src = which == 0 ? h->centre : h->face[which - 1];
+  const size_t size = which == 0 ? (size_t)NCF * c.nx * c.ny : (src ? (size_t)NFF * nf[which - 1] : 0);
+  if (n_out) *n_out = size;
+  if (size == 0 || (!out && n == 0)) return GRHD2_OK;
+  if (!out || n < size) return fail(h, GRHD2_ERR_ARG, "metric table %d holds %zu doubles; out holds %zu", which, size, n);
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  CUDA_TRY(h, cudaMemcpyAsync(out, src, size * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return GRHD2_OK;
 }
 

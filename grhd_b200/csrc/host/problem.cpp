@@ -6,6 +6,7 @@
 // metrics (metrics.f90:209-1242), the initial conditions (conditions.f90:26-582) and the
 // perturbations (conditions.f90:585-768).  Nothing here runs per stage.
 #include "grhd2_host.h"
+#include "metric_eval.h"
 
 #include <cctype>
 #include <cfloat>
@@ -60,353 +61,21 @@ struct Params {
 };
 
 // ------------------------------------------------------------------------------------
-// metrics.f90: analytic 3+1 quantities.  gamma(3,3) Fortran order g[(a-1)+3(b-1)],
-// gmunu(0:3,0:3) -> gm[mu+4nu], chris(0:3,0:3,0:3) -> ch[l+4m+16n], dg(0:3,0:3,1:3) ->
-// dg[m+4n+16(d-1)], dlnalpha(0:3).
+// metrics.f90: the analytic 3+1 quantities and the set_metric_type dispatch live in
+// metric_eval.h, which the device metric-cache build compiles too.
 // ------------------------------------------------------------------------------------
-struct MetricOut {
-  double alpha = 0, beta[3] = {0, 0, 0}, gamma[9] = {0}, gmunu[16] = {0}, det = 0, dlna[4] = {0};
-};
-#define GG(a, b) m.gamma[((a) - 1) + 3 * ((b) - 1)]
-#define GM(a, b) m.gmunu[(a) + 4 * (b)]
-#define CH(l, a, b) ch[(l) + 4 * (a) + 16 * (b)]
-#define DG(a, b, d) dg[(a) + 4 * (b) + 16 * ((d) - 1)]
+using grhd2_metric::MetricOut;
 
 inline double sq(double x) { return x * x; }
 
-// metrics.f90:209-239
-void metric_minkowski(MetricOut &m) {
-  m.alpha = 1.0;
-  GG(1, 1) = 1.0; GG(2, 2) = 1.0; GG(3, 3) = 1.0;
-  m.det = 1.0;
-  GM(0, 0) = -1.0; GM(1, 1) = 1.0; GM(2, 2) = 1.0; GM(3, 3) = 1.0;
+grhd2_metric::Kind metric_kind(const Params &P) {
+  return grhd2_metric::Kind{P.metric, P.geom, P.log_r ? 1 : 0, P.ny, P.bh_mass, P.a_spin};
 }
-// metrics.f90:419-450
-void metric_cylindrical(double x, MetricOut &m) {
-  m.alpha = 1.0;
-  GG(1, 1) = 1.0; GG(2, 2) = sq(x); GG(3, 3) = 1.0;
-  m.det = sq(x);
-  GM(0, 0) = -1.0; GM(1, 1) = 1.0; GM(2, 2) = 1.0 / std::fmax(sq(x), 1.0e-20); GM(3, 3) = 1.0;
-}
-void chris_cylindrical(double x, double *ch) {
-  CH(1, 2, 2) = -x;
-  CH(2, 1, 2) = 1.0 / std::fmax(x, 1.0e-15);
-  CH(2, 2, 1) = 1.0 / std::fmax(x, 1.0e-15);
-}
-void derivs_cylindrical(double x, double *dg) { DG(2, 2, 1) = 2.0 * x; }
-// metrics.f90:265-333
-void metric_mink_sph_phys(double r, double th, MetricOut &m) {
-  double r2 = sq(r), s = std::sin(th), s2 = sq(s);
-  m.alpha = 1.0;
-  GG(1, 1) = 1.0; GG(2, 2) = r2; GG(3, 3) = r2 * s2;
-  m.det = r2 * r2 * s2;
-  GM(0, 0) = -1.0; GM(1, 1) = 1.0; GM(2, 2) = 1.0 / r2; GM(3, 3) = 1.0 / std::fmax(r2 * s2, 1.0e-30);
-}
-void derivs_mink_sph_phys(double r, double th, int ny, double *dg) {
-  double s = std::sin(th), c = std::cos(th);
-  DG(2, 2, 1) = 2.0 * r;
-  DG(3, 3, 1) = 2.0 * r * sq(s);
-  DG(3, 3, 2) = 2.0 * sq(r) * s * c;
-  if (ny == 1) for (int a = 0; a < 16; ++a) dg[a + 16] = 0.0;
-}
-void chris_mink_sph_phys(double r, double th, double *ch) {
-  double s = std::sin(th), c = std::cos(th);
-  double safe = std::copysign(std::fmax(std::fabs(s), 1.0e-20), s);
-  CH(1, 2, 2) = -r;
-  CH(1, 3, 3) = -r * sq(s);
-  CH(2, 1, 2) = 1.0 / r; CH(2, 2, 1) = CH(2, 1, 2);
-  CH(2, 3, 3) = -s * c;
-  CH(3, 1, 3) = 1.0 / r; CH(3, 3, 1) = CH(3, 1, 3);
-  CH(3, 2, 3) = c / safe; CH(3, 3, 2) = CH(3, 2, 3);
-}
-// metrics.f90:338-411
-void metric_mink_sph_log(double x, double th, MetricOut &m) {
-  double r = std::exp(x), r2 = sq(r), s = std::sin(th), s2 = sq(s);
-  m.alpha = 1.0;
-  GG(1, 1) = r2; GG(2, 2) = r2; GG(3, 3) = r2 * s2;
-  m.det = r2 * r2 * r2 * s2;
-  GM(0, 0) = -1.0; GM(1, 1) = 1.0 / r2; GM(2, 2) = 1.0 / r2; GM(3, 3) = 1.0 / std::fmax(r2 * s2, 1.0e-30);
-}
-void derivs_mink_sph_log(double x, double th, int ny, double *dg) {
-  double r2 = std::exp(2.0 * x), s = std::sin(th), c = std::cos(th);
-  DG(1, 1, 1) = 2.0 * r2;
-  DG(2, 2, 1) = 2.0 * r2;
-  DG(3, 3, 1) = 2.0 * r2 * sq(s);
-  DG(3, 3, 2) = 2.0 * r2 * s * c;
-  if (ny == 1) for (int a = 0; a < 16; ++a) dg[a + 16] = 0.0;
-}
-void chris_mink_sph_log(double th, double *ch) {
-  double s = std::sin(th), c = std::cos(th);
-  double safe = std::copysign(std::fmax(std::fabs(s), 1.0e-20), s);
-  CH(1, 1, 1) = 1.0;
-  CH(1, 2, 2) = -1.0;
-  CH(1, 3, 3) = -sq(s);
-  CH(2, 1, 2) = 1.0; CH(2, 2, 1) = CH(2, 1, 2);
-  CH(2, 3, 3) = -s * c;
-  CH(3, 1, 3) = 1.0; CH(3, 3, 1) = CH(3, 1, 3);
-  CH(3, 2, 3) = c / safe; CH(3, 3, 2) = CH(3, 2, 3);
-}
-// metrics.f90:492-610 (EF, physical r)
-void metric_ef_phys(double r, double th, double M, bool want_gmunu, MetricOut &m) {
-  double s = std::sin(th);
-  m.alpha = 1.0 / std::sqrt(1.0 + 2.0 * M / r);
-  m.beta[0] = 2.0 * M / r / (1.0 + 2.0 * M / r);
-  double g11 = 1.0 + 2.0 * M / r, g22 = sq(r), g33 = sq(r) * sq(s);
-  m.det = g11 * g22 * g33;
-  GG(1, 1) = g11; GG(2, 2) = g22; GG(3, 3) = g33;
-  if (want_gmunu) {
-    GM(0, 0) = -1.0 / sq(m.alpha);
-    for (int d = 1; d <= 3; ++d) { GM(0, d) = m.beta[d - 1] / sq(m.alpha); GM(d, 0) = GM(0, d); }
-    GM(1, 1) = 1.0 / g11 - sq(m.beta[0]) / sq(m.alpha);
-    GM(2, 2) = 1.0 / g22 - sq(m.beta[1]) / sq(m.alpha);
-    GM(3, 3) = 1.0 / g33 - sq(m.beta[2]) / sq(m.alpha);
-  }
-  m.dlna[1] = M / (sq(r) + 2.0 * M * r);
-}
-void chris_ef_phys(double r, double th, double M, double *ch) {
-  double s = std::sin(th), c = std::cos(th);
-  double safe = std::copysign(std::fmax(std::fabs(s), 1.0e-20), s);
-  double r3 = r * r * r;
-  CH(0, 0, 0) = 2.0 * sq(M) / r3;
-  CH(0, 0, 1) = M * (1.0 + 2.0 * M / r) / sq(r);
-  CH(0, 1, 0) = CH(0, 0, 1);
-  CH(0, 1, 1) = 2.0 * M * (1.0 + M / r) / sq(r);
-  CH(0, 2, 2) = -2.0 * M;
-  CH(0, 3, 3) = CH(0, 2, 2) * sq(s);
-  CH(1, 0, 0) = M / sq(r) * (1.0 - 2.0 * M / r);
-  CH(1, 0, 1) = -CH(0, 0, 0);
-  CH(1, 1, 0) = CH(1, 0, 1);
-  CH(1, 1, 1) = -CH(0, 0, 1);
-  CH(1, 2, 2) = 2.0 * M - r;
-  CH(1, 3, 3) = CH(1, 2, 2) * sq(s);
-  CH(2, 1, 2) = 1.0 / r; CH(2, 2, 1) = CH(2, 1, 2);
-  CH(2, 3, 3) = -s * c;
-  CH(3, 1, 3) = 1.0 / r; CH(3, 3, 1) = CH(3, 1, 3);
-  CH(3, 2, 3) = c / safe; CH(3, 3, 2) = CH(3, 2, 3);
-}
-void derivs_ef_phys(double r, double th, double M, int ny, double *dg) {
-  double s = std::sin(th), c = std::cos(th);
-  DG(0, 0, 1) = -2.0 * M / sq(r);
-  DG(0, 1, 1) = -2.0 * M / sq(r); DG(1, 0, 1) = DG(0, 1, 1);
-  DG(1, 1, 1) = -2.0 * M / sq(r);
-  DG(2, 2, 1) = 2.0 * r;
-  DG(3, 3, 1) = 2.0 * r * sq(s);
-  DG(3, 3, 2) = sq(r) * 2.0 * s * c;
-  if (ny == 1) for (int a = 0; a < 16; ++a) dg[a + 16] = 0.0;
-}
-// metrics.f90:612-746 (EF, x = ln r)
-void metric_ef_log(double x, double th, double M, bool want_gmunu, MetricOut &m) {
-  double r = std::exp(x), s = std::sin(th);
-  m.alpha = 1.0 / std::sqrt(1.0 + 2.0 * M / r);
-  m.beta[0] = (2.0 * M / r / (1.0 + 2.0 * M / r)) / r;
-  double g11 = (1.0 + 2.0 * M / r) * sq(r), g22 = sq(r), g33 = sq(r) * sq(s);
-  m.det = g11 * g22 * g33;
-  GG(1, 1) = g11; GG(2, 2) = g22; GG(3, 3) = g33;
-  if (want_gmunu) {
-    GM(0, 0) = -1.0 / sq(m.alpha);
-    for (int d = 1; d <= 3; ++d) { GM(0, d) = m.beta[d - 1] / sq(m.alpha); GM(d, 0) = GM(0, d); }
-    GM(1, 1) = 1.0 / g11 - sq(m.beta[0]) / sq(m.alpha);
-    GM(2, 2) = 1.0 / g22 - sq(m.beta[1]) / sq(m.alpha);
-    GM(3, 3) = 1.0 / g33 - sq(m.beta[2]) / sq(m.alpha);
-  }
-  m.dlna[1] = M / (r + 2.0 * M);
-}
-void chris_ef_log(double x, double th, double M, double *ch) {
-  double r = std::exp(x), s = std::sin(th), c = std::cos(th);
-  double safe = std::copysign(std::fmax(std::fabs(s), 1.0e-20), s);
-  double r3 = r * r * r;
-  CH(0, 0, 0) = 2.0 * sq(M) / r3;
-  CH(0, 0, 1) = M * (1.0 + 2.0 * M / r) / r;
-  CH(0, 1, 0) = CH(0, 0, 1);
-  CH(0, 1, 1) = 2.0 * M * (1.0 + M / r);
-  CH(0, 2, 2) = -2.0 * M;
-  CH(0, 3, 3) = CH(0, 2, 2) * sq(s);
-  CH(1, 0, 0) = M / r3 * (1.0 - 2.0 * M / r);
-  CH(1, 0, 1) = -2.0 * sq(M) / r3;
-  CH(1, 1, 0) = CH(1, 0, 1);
-  CH(1, 1, 1) = 1.0 - M / r - 2.0 * sq(M) / sq(r);
-  CH(1, 2, 2) = 2.0 * M / r - 1.0;
-  CH(1, 3, 3) = CH(1, 2, 2) * sq(s);
-  CH(2, 1, 2) = 1.0; CH(2, 2, 1) = CH(2, 1, 2);
-  CH(2, 3, 3) = -s * c;
-  CH(3, 1, 3) = 1.0; CH(3, 3, 1) = CH(3, 1, 3);
-  CH(3, 2, 3) = c / safe; CH(3, 3, 2) = CH(3, 2, 3);
-}
-void derivs_ef_log(double x, double th, double M, int ny, double *dg) {
-  double r = std::exp(x), s = std::sin(th), c = std::cos(th);
-  DG(0, 0, 1) = -2.0 * M / r;
-  DG(0, 1, 1) = 0.0; DG(1, 0, 1) = DG(0, 1, 1);
-  DG(1, 1, 1) = 2.0 * sq(r) + 2.0 * M * r;
-  DG(2, 2, 1) = 2.0 * sq(r);
-  DG(3, 3, 1) = 2.0 * sq(r) * sq(s);
-  DG(3, 3, 2) = 2.0 * sq(r) * s * c;
-  if (ny == 1) for (int a = 0; a < 16; ++a) dg[a + 16] = 0.0;
-}
-// metrics.f90:753-921 (KS, physical r)
-void metric_ks_phys(double r, double th, double M, double a, bool want_gmunu, MetricOut &m) {
-  double s = std::sin(th), c = std::cos(th), s2 = sq(s), c2 = sq(c);
-  double Sigma = sq(r) + sq(a) * c2, H = M * r / Sigma, Delta = sq(r) - 2.0 * M * r + sq(a);
-  m.alpha = 1.0 / std::sqrt(1.0 + 2.0 * H);
-  m.beta[0] = 2.0 * H / (1.0 + 2.0 * H);
-  GG(1, 1) = 1.0 + 2.0 * H;
-  GG(1, 3) = -a * (1.0 + 2.0 * H) * s2; GG(3, 1) = GG(1, 3);
-  GG(2, 2) = Sigma;
-  GG(3, 3) = (sq(r) + sq(a) + 2.0 * H * sq(a) * s2) * s2;
-  m.det = sq(Sigma) * s2 * (1.0 + 2.0 * H);
-  if (want_gmunu) {
-    GM(0, 0) = -(1.0 + 2.0 * H);
-    GM(0, 1) = 2.0 * H; GM(1, 0) = GM(0, 1);
-    GM(1, 1) = Delta / Sigma;
-    GM(1, 3) = a / Sigma; GM(3, 1) = GM(1, 3);
-    GM(2, 2) = 1.0 / Sigma;
-    GM(3, 3) = (std::fabs(s) > 1.0e-15) ? 1.0 / (Sigma * s2) : 1.0 / (Sigma * 1.0e-30);
-  }
-  double dH_dr = M * (sq(a) * c2 - sq(r)) / sq(Sigma);
-  double dH_dth = 2.0 * M * r * sq(a) * s * c / sq(Sigma);
-  m.dlna[1] = -dH_dr / (1.0 + 2.0 * H);
-  m.dlna[2] = -dH_dth / (1.0 + 2.0 * H);
-}
-void derivs_ks_phys(double r, double th, double M, double a, int ny, double *dg) {
-  double s = std::sin(th), c = std::cos(th), s2 = sq(s), c2 = sq(c);
-  double Sigma = sq(r) + sq(a) * c2, H = M * r / Sigma;
-  double dS_dr = 2.0 * r, dS_dth = -2.0 * sq(a) * s * c;
-  double dH_dr = M * (sq(a) * c2 - sq(r)) / sq(Sigma);
-  double dH_dth = 2.0 * M * r * sq(a) * s * c / sq(Sigma);
-  DG(0, 0, 1) = 2.0 * dH_dr;
-  DG(0, 1, 1) = 2.0 * dH_dr; DG(1, 0, 1) = DG(0, 1, 1);
-  DG(0, 3, 1) = -2.0 * a * s2 * dH_dr; DG(3, 0, 1) = DG(0, 3, 1);
-  DG(1, 1, 1) = 2.0 * dH_dr;
-  DG(1, 3, 1) = -a * s2 * (2.0 * dH_dr); DG(3, 1, 1) = DG(1, 3, 1);
-  DG(2, 2, 1) = dS_dr;
-  DG(3, 3, 1) = 2.0 * r * s2 + 2.0 * sq(a) * sq(s2) * dH_dr;
-  DG(0, 0, 2) = 2.0 * dH_dth;
-  DG(0, 1, 2) = 2.0 * dH_dth; DG(1, 0, 2) = DG(0, 1, 2);
-  DG(0, 3, 2) = -2.0 * a * (s2 * dH_dth + 2.0 * H * s * c); DG(3, 0, 2) = DG(0, 3, 2);
-  DG(1, 1, 2) = 2.0 * dH_dth;
-  DG(1, 3, 2) = -a * ((1.0 + 2.0 * H) * 2.0 * s * c + s2 * 2.0 * dH_dth); DG(3, 1, 2) = DG(1, 3, 2);
-  DG(2, 2, 2) = dS_dth;
-  DG(3, 3, 2) = 2.0 * (sq(r) + sq(a)) * s * c + 2.0 * sq(a) * sq(s2) * dH_dth + 8.0 * sq(a) * H * s * c * s2;
-  if (ny == 1) for (int q = 0; q < 16; ++q) dg[q + 16] = 0.0;
-}
-// metrics.f90:998-1180 (KS, x = ln r)
-void metric_ks_log(double x, double th, double M, double a, bool want_gmunu, MetricOut &m) {
-  double r = std::exp(x), s = std::sin(th), c = std::cos(th), s2 = sq(s), c2 = sq(c);
-  double Sigma = sq(r) + sq(a) * c2, H = M * r / Sigma, Delta = sq(r) - 2.0 * M * r + sq(a);
-  m.alpha = 1.0 / std::sqrt(1.0 + 2.0 * H);
-  m.beta[0] = (2.0 * H / (1.0 + 2.0 * H)) / r;
-  GG(1, 1) = (1.0 + 2.0 * H) * sq(r);
-  GG(1, 3) = -a * (1.0 + 2.0 * H) * s2 * r; GG(3, 1) = GG(1, 3);
-  GG(2, 2) = Sigma;
-  GG(3, 3) = (sq(r) + sq(a) + 2.0 * H * sq(a) * s2) * s2;
-  m.det = (sq(Sigma) * s2 * (1.0 + 2.0 * H)) * sq(r);
-  if (want_gmunu) {
-    GM(0, 0) = -(1.0 + 2.0 * H);
-    GM(0, 1) = (2.0 * H) / r; GM(1, 0) = GM(0, 1);
-    GM(1, 1) = (Delta / Sigma) / sq(r);
-    GM(1, 3) = (a / Sigma) / r; GM(3, 1) = GM(1, 3);
-    GM(2, 2) = 1.0 / Sigma;
-    GM(3, 3) = (std::fabs(s) > 1.0e-15) ? 1.0 / (Sigma * s2) : 1.0 / (Sigma * 1.0e-30);
-  }
-  double dH_dr = M * (sq(a) * c2 - sq(r)) / sq(Sigma);
-  double dH_dth = 2.0 * M * r * sq(a) * s * c / sq(Sigma);
-  m.dlna[1] = -(dH_dr * r) / (1.0 + 2.0 * H);
-  m.dlna[2] = -dH_dth / (1.0 + 2.0 * H);
-}
-void derivs_ks_log(double x, double th, double M, double a, int ny, double *dg) {
-  double r = std::exp(x), s = std::sin(th), c = std::cos(th), s2 = sq(s), c2 = sq(c);
-  double Sigma = sq(r) + sq(a) * c2, H = M * r / Sigma;
-  double dS_dth = -2.0 * sq(a) * s * c;
-  double dH_dr = M * (sq(a) * c2 - sq(r)) / sq(Sigma);
-  double dH_dth = 2.0 * M * r * sq(a) * s * c / sq(Sigma);
-  double g_tr = 2.0 * H, g_rr = 1.0 + 2.0 * H, g_rphi = -a * (1.0 + 2.0 * H) * s2;
-  double r3 = r * r * r;
-  DG(0, 0, 1) = r * (2.0 * dH_dr);
-  DG(0, 1, 1) = r * g_tr + sq(r) * (2.0 * dH_dr); DG(1, 0, 1) = DG(0, 1, 1);
-  DG(0, 3, 1) = r * (-2.0 * a * s2 * dH_dr); DG(3, 0, 1) = DG(0, 3, 1);
-  DG(1, 1, 1) = 2.0 * sq(r) * g_rr + r3 * (2.0 * dH_dr);
-  DG(1, 3, 1) = r * g_rphi + sq(r) * (-2.0 * a * s2 * dH_dr); DG(3, 1, 1) = DG(1, 3, 1);
-  DG(2, 2, 1) = 2.0 * sq(r);
-  DG(3, 3, 1) = r * (2.0 * r * s2 + 2.0 * sq(a) * sq(s2) * dH_dr);
-  DG(0, 0, 2) = 2.0 * dH_dth;
-  DG(0, 1, 2) = r * (2.0 * dH_dth); DG(1, 0, 2) = DG(0, 1, 2);
-  DG(0, 3, 2) = -2.0 * a * (s2 * dH_dth + 2.0 * H * s * c); DG(3, 0, 2) = DG(0, 3, 2);
-  DG(1, 1, 2) = sq(r) * (2.0 * dH_dth);
-  DG(1, 3, 2) = r * (-a * ((1.0 + 2.0 * H) * 2.0 * s * c + s2 * 2.0 * dH_dth)); DG(3, 1, 2) = DG(1, 3, 2);
-  DG(2, 2, 2) = dS_dth;
-  DG(3, 3, 2) = 2.0 * (sq(r) + sq(a)) * s * c + 2.0 * sq(a) * sq(s2) * dH_dth + 8.0 * sq(a) * H * s * c * s2;
-  if (ny == 1) for (int q = 0; q < 16; ++q) dg[q + 16] = 0.0;
-}
-// metrics.f90:926-990 / 1186-1242: Gamma^l_{mn} = 1/2 g^{lr}(d_m g_rn + d_n g_rm - d_r g_mn)
-void chris_from_dg(const double *gmunu, const double *dg, double *ch) {
-  for (int l = 0; l <= 3; ++l)
-    for (int mu = 0; mu <= 3; ++mu)
-      for (int nu = mu; nu <= 3; ++nu) {
-        for (int rho = 0; rho <= 3; ++rho) {
-          double dm = 0.0, dn = 0.0, dr = 0.0;
-          if (mu == 1) dm = DG(rho, nu, 1); else if (mu == 2) dm = DG(rho, nu, 2);
-          if (nu == 1) dn = DG(rho, mu, 1); else if (nu == 2) dn = DG(rho, mu, 2);
-          if (rho == 1) dr = DG(mu, nu, 1); else if (rho == 2) dr = DG(mu, nu, 2);
-          CH(l, mu, nu) = CH(l, mu, nu) + 0.5 * gmunu[l + 4 * rho] * (dm + dn - dr);
-        }
-        if (mu != nu) CH(l, nu, mu) = CH(l, mu, nu);
-      }
-}
-#undef GG
-#undef GM
-#undef CH
-#undef DG
-
-// set_metric_type dispatch (metrics.f90:94-201)
 void eval_metric(const Params &P, double x, double y, bool want_gmunu, MetricOut &m) {
-  m = MetricOut();
-  switch (P.metric) {
-  case MINK:
-    if (P.geom == CART) metric_minkowski(m);
-    else if (P.geom == CYL) metric_cylindrical(x, m);
-    else if (P.log_r) metric_mink_sph_log(x, y, m);
-    else metric_mink_sph_phys(x, y, m);
-    break;
-  case EF:
-    if (P.log_r) metric_ef_log(x, y, P.bh_mass, want_gmunu, m);
-    else metric_ef_phys(x, y, P.bh_mass, want_gmunu, m);
-    break;
-  case KS:
-    if (P.log_r) metric_ks_log(x, y, P.bh_mass, P.a_spin, want_gmunu, m);
-    else metric_ks_phys(x, y, P.bh_mass, P.a_spin, want_gmunu, m);
-    break;
-  }
+  grhd2_metric::eval_metric(metric_kind(P), x, y, want_gmunu, m);
 }
 void eval_chris_dg(const Params &P, double x, double y, double *ch, double *dg) {
-  for (int q = 0; q < 64; ++q) ch[q] = 0.0;
-  for (int q = 0; q < 48; ++q) dg[q] = 0.0;
-  switch (P.metric) {
-  case MINK:
-    if (P.geom == CART) {
-    } else if (P.geom == CYL) {
-      chris_cylindrical(x, ch); derivs_cylindrical(x, dg);
-    } else if (P.log_r) {
-      chris_mink_sph_log(y, ch); derivs_mink_sph_log(x, y, P.ny, dg);
-    } else {
-      chris_mink_sph_phys(x, y, ch); derivs_mink_sph_phys(x, y, P.ny, dg);
-    }
-    break;
-  case EF:
-    if (P.log_r) { chris_ef_log(x, y, P.bh_mass, ch); derivs_ef_log(x, y, P.bh_mass, P.ny, dg); }
-    else { chris_ef_phys(x, y, P.bh_mass, ch); derivs_ef_phys(x, y, P.bh_mass, P.ny, dg); }
-    break;
-  case KS: {
-    MetricOut m;
-    if (P.log_r) {
-      metric_ks_log(x, y, P.bh_mass, P.a_spin, true, m);
-      derivs_ks_log(x, y, P.bh_mass, P.a_spin, P.ny, dg);
-    } else {
-      metric_ks_phys(x, y, P.bh_mass, P.a_spin, true, m);
-      derivs_ks_phys(x, y, P.bh_mass, P.a_spin, P.ny, dg);
-    }
-    chris_from_dg(m.gmunu, dg, ch);
-    break;
-  }
-  }
+  grhd2_metric::eval_chris_dg(metric_kind(P), x, y, ch, dg);
 }
 
 }  // namespace
@@ -424,6 +93,7 @@ struct grhd2_problem {
   std::vector<double> p;  // (5,-g:nx+g,-g:ny+g,-g:nz+g)
   std::vector<double> michel_injector, dust_outer;
   double fm_l = 0, fm_w_in = 0;
+  bool metric_cache = true;  // false: the tables are built on the device instead
 
   size_t pidx(int v, int i, int j, int k) const {
     const int g = P.nghost;
@@ -877,6 +547,9 @@ bool fm_state(const Params &P, double r, double r_in, double K, double l_ang, do
   return true;
 }
 
+void build_metric_cache(grhd2_problem &pb);
+void set_initial_conditions(grhd2_problem &pb);
+
 void build(grhd2_problem &pb) {
   Params &P = pb.P;
   const int nx = P.nx, ny = P.ny, nz = P.nz, g = P.nghost;
@@ -896,6 +569,13 @@ void build(grhd2_problem &pb) {
   for (int k = -g; k <= nz + g; ++k) pb.Z(k) = P.z_min + ((double)k - 0.5) * pb.dz;
 
   // precalculate_metric_cache, initialization.f90:265-391 (k = 1 slice)
+  if (pb.metric_cache) build_metric_cache(pb);
+  set_initial_conditions(pb);
+}
+
+void build_metric_cache(grhd2_problem &pb) {
+  const Params &P = pb.P;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
   const size_t nc = (size_t)nx * ny;
   pb.alpha_c.assign(nc, 0); pb.beta_c.assign(3 * nc, 0); pb.gamma_c.assign(9 * nc, 0);
   pb.gamma_inv_c.assign(9 * nc, 0); pb.gmunu_c.assign(16 * nc, 0); pb.sqg_c.assign(nc, 0);
@@ -964,7 +644,11 @@ void build(grhd2_problem &pb) {
         pb.s_fz[f] = std::sqrt(m.det);
       }
   }
+}
 
+void set_initial_conditions(grhd2_problem &pb) {
+  const Params &P = pb.P;
+  const int nx = P.nx, ny = P.ny, nz = P.nz, g = P.nghost;
   // set_initial_conditions, conditions.f90:26-214
   pb.p.assign((size_t)5 * (nx + 2 * g + 1) * (ny + 2 * g + 1) * (nz + 2 * g + 1), 0.0);
   auto Pv = [&](int v, int i, int j, int k) -> double & { return pb.p[pb.pidx(v, i, j, k)]; };
@@ -1123,15 +807,22 @@ void build(grhd2_problem &pb) {
   case 10: case 11: case 12: {
     double r_in = P.fm_rin * P.bh_mass, r_mx = P.fm_rmax * P.bh_mass;
     if (!fm_prepare(P, r_in, r_mx, pb.fm_l, pb.fm_w_in)) fail("invalid Fishbone-Moncrief model parameters");
-    for (int k = 1; k <= nz; ++k)
-      for (int j = 1; j <= ny; ++j)
-        for (int i = 1; i <= nx; ++i) {
-          double r = P.log_r ? std::exp(pb.X(i)) : pb.X(i);
-          size_t c = (size_t)(i - 1) + (size_t)nx * (j - 1);
-          double pc[5];
-          fm_state(P, r, r_in, P.fm_k, pb.fm_l, pb.fm_w_in, pb.alpha_c[c], &pb.beta_c[3 * c], &pb.gamma_c[9 * c], pc);
+    // the centre metric from the cache, or evaluated here when the cache is built on the
+    // device (the same function at the same point: the same values)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double r = P.log_r ? std::exp(pb.X(i)) : pb.X(i);
+        const size_t c = (size_t)(i - 1) + (size_t)nx * (j - 1);
+        MetricOut m;
+        if (!pb.metric_cache) eval_metric(P, pb.X(i), pb.Y(j), false, m);
+        const double alpha = pb.metric_cache ? pb.alpha_c[c] : m.alpha;
+        const double *beta = pb.metric_cache ? &pb.beta_c[3 * c] : m.beta;
+        const double *gamma = pb.metric_cache ? &pb.gamma_c[9 * c] : m.gamma;
+        double pc[5];
+        fm_state(P, r, r_in, P.fm_k, pb.fm_l, pb.fm_w_in, alpha, beta, gamma, pc);
+        for (int k = 1; k <= nz; ++k)
           for (int v = 0; v < 5; ++v) Pv(v, i, j, k) = pc[v];
-        }
+      }
     break;
   }
   }
@@ -1157,10 +848,19 @@ struct SplitMix64 {
 extern "C" {
 
 int grhd2_problem_create(const char *par_text, grhd2_problem **out, char *err, int errlen) {
+  return grhd2_problem_create_ex(par_text, 0u, out, err, errlen);
+}
+
+int grhd2_problem_create_ex(const char *par_text, uint32_t flags, grhd2_problem **out, char *err, int errlen) {
   if (!par_text || !out) return GRHD2_ERR_ARG;
   *out = nullptr;
+  if (flags & ~(uint32_t)GRHD2_PROBLEM_NO_METRIC_CACHE) {
+    if (err && errlen > 0) std::snprintf(err, (size_t)errlen, "unknown problem flags 0x%x", (unsigned)flags);
+    return GRHD2_ERR_ARG;
+  }
   grhd2_problem *pb = new (std::nothrow) grhd2_problem();
   if (!pb) return GRHD2_ERR_NOMEM;
+  pb->metric_cache = !(flags & GRHD2_PROBLEM_NO_METRIC_CACHE);
   try {
     read_par(par_text, pb->P);
     validate(pb->P);
@@ -1196,6 +896,11 @@ int grhd2_problem_config(const grhd2_problem *pb, int32_t precision_policy, grhd
 int grhd2_problem_metric(const grhd2_problem *pb, grhd2_gpu_metric_view *mv) {
   if (!pb || !mv) return GRHD2_ERR_ARG;
   std::memset(mv, 0, sizeof *mv);
+  if (!pb->metric_cache) {  // the face coordinates only
+    mv->x_face = pb->x_face.data();
+    mv->y_face = pb->y_face.data();
+    return GRHD2_ERR_STATE;
+  }
   mv->alpha_c = pb->alpha_c.data(); mv->beta_c = pb->beta_c.data(); mv->gamma_c = pb->gamma_c.data();
   mv->gamma_inv_c = pb->gamma_inv_c.data(); mv->gmunu_c = pb->gmunu_c.data(); mv->sqrt_gamma_c = pb->sqg_c.data();
   mv->chris_c = pb->chris_c.data(); mv->dg_c = pb->dg_c.data(); mv->dlna_c = pb->dlna_c.data();

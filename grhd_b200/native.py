@@ -38,6 +38,11 @@ class MetricView(C.Structure):
         "x_face", "y_face")]
 
 
+class MetricParams(C.Structure):
+    """grhd2_gpu_metric_params (include/grhd2_gpu.h)."""
+    _fields_ = [(n, C.c_double) for n in ("bh_mass", "a_spin", "x_min", "y_min")]
+
+
 class BcView(C.Structure):
     """grhd2_gpu_bc_view (include/grhd2_gpu.h)."""
     _fields_ = [("michel_injector", c_double_p), ("dust_outer", c_double_p),
@@ -81,6 +86,8 @@ _VP = C.c_void_p
 GPU_SYMBOLS = {
     "grhd2_gpu_create": (C.c_int, [C.POINTER(GpuConfig), C.POINTER(_VP)]),
     "grhd2_gpu_set_metric": (C.c_int, [_VP, C.POINTER(MetricView)]),
+    "grhd2_gpu_set_metric_analytic": (C.c_int, [_VP, C.POINTER(MetricParams)]),
+    "grhd2_gpu_metric_table": (C.c_int, [_VP, C.c_int32, c_double_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "grhd2_gpu_set_bc_data": (C.c_int, [_VP, C.POINTER(BcView)]),
     "grhd2_gpu_upload": (C.c_int, [_VP, c_double_p, c_double_p]),
     "grhd2_gpu_prim_to_cons_all": (C.c_int, [_VP]),
@@ -146,6 +153,7 @@ GPU_SYMBOLS = {
 
 HOST_SYMBOLS = {
     "grhd2_problem_create": (C.c_int, [C.c_char_p, C.POINTER(_VP), C.c_char_p, C.c_int]),
+    "grhd2_problem_create_ex": (C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(_VP), C.c_char_p, C.c_int]),
     "grhd2_problem_destroy": (None, [_VP]),
     "grhd2_problem_config": (C.c_int, [_VP, C.c_int32, C.POINTER(GpuConfig)]),
     "grhd2_problem_metric": (C.c_int, [_VP, C.POINTER(MetricView)]),

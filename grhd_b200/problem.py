@@ -32,24 +32,27 @@ def par_text(problem: str, **keys) -> str:
 class Problem:
     """Host-side problem: grid, metric tables, boundary data, initial primitives."""
 
-    def __init__(self, text: str):
+    def __init__(self, text: str, metric_cache: bool = True):
+        """metric_cache=False builds no host metric cache (grhd2_problem_create_ex with
+        GRHD2_PROBLEM_NO_METRIC_CACHE): for grids whose tables are built on the device."""
         lib = N.host_lib()
         h = C.c_void_p()
         err = C.create_string_buffer(512)
-        rc = lib.grhd2_problem_create(text.encode(), C.byref(h), err, 512)
+        rc = lib.grhd2_problem_create_ex(text.encode(), 0 if metric_cache else 1, C.byref(h), err, 512)
         if rc != 0:
             raise ValueError(f"invalid problem ({rc}): {err.value.decode()}")
         self._lib = lib
         self._h = h
         self.text = text
+        self.metric_cache = metric_cache
         info = N.ProblemInfo()
         lib.grhd2_problem_info_get(h, C.byref(info))
         self.info = info
         self.nx, self.ny, self.nz, self.ng = info.nx, info.ny, info.nz, info.nghost
 
     @classmethod
-    def from_keys(cls, problem: str, **keys) -> "Problem":
-        return cls(par_text(problem, **keys))
+    def from_keys(cls, problem: str, metric_cache: bool = True, **keys) -> "Problem":
+        return cls(par_text(problem, **keys), metric_cache=metric_cache)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -64,9 +67,16 @@ class Problem:
         return c
 
     def metric_view(self) -> N.MetricView:
+        if not self.metric_cache:
+            raise RuntimeError("this problem was built without a host metric cache (metric_cache=False)")
         m = N.MetricView()
         self._lib.grhd2_problem_metric(self._h, C.byref(m))
         return m
+
+    def metric_params(self) -> N.MetricParams:
+        """What grhd2_gpu_set_metric_analytic needs beyond the configuration."""
+        i = self.info
+        return N.MetricParams(bh_mass=i.bh_mass, a_spin=i.a_spin, x_min=i.x_min, y_min=i.y_min)
 
     def bc_view(self) -> N.BcView:
         b = N.BcView()
@@ -132,7 +142,9 @@ class Problem:
         x, _, _ = self.coords()
         g = self.ng
         xc = x[g + 1:g + 1 + self.nx]
-        xf = np.ctypeslib.as_array(self.metric_view().x_face, shape=(self.nx + 1,))
+        m = N.MetricView()
+        self._lib.grhd2_problem_metric(self._h, C.byref(m))  # x_face is set with or without the cache
+        xf = np.ctypeslib.as_array(m.x_face, shape=(self.nx + 1,))
         if r_h < xf[0]:
             return 1
         if r_h > xf[self.nx]:

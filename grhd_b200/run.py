@@ -140,6 +140,8 @@ def main(argv=None):
                     help="run the problem in FP64 and mixed from the same state to --final-time (or --steps) "
                          "and report the mixed-vs-FP64 L1 (and the Michel L1 against the analytic profile)")
     ap.add_argument("--final-time", type=float, default=None)
+    ap.add_argument("--metric", choices=["host", "device"], default="host",
+                    help="upload the host-built metric cache, or build it on the device")
     args, rest = ap.parse_known_args(argv)
     overrides = _parse_overrides(rest)
     from .problem import Problem
@@ -169,7 +171,7 @@ def main(argv=None):
             if pr.info.perturbation_type and pr.info.perturbation_time <= 0.0:
                 pr.perturb(q)
         gr = GpuGrid(pr, precision=args.precision, upload_initial=False,
-                     stream=grids[0].stream_ptr if grids else None)
+                     stream=grids[0].stream_ptr if grids else None, metric=args.metric)
         gr.upload(p=q)
         gr.prim_to_cons()
         grids.append(gr)
@@ -196,7 +198,8 @@ def main(argv=None):
     out = {"cells": cells, "grids": len(grids), "steps": args.steps, "dt": g.cfl(),
            "ms_per_step": el / args.steps * 1e3, "zone_updates_per_s": cells * args.steps / el,
            "kernels": prof, "counters": g.counters(), "flux_variant": tuned or args.flux,
-           "stage_groups": batch.stage_groups}
+           "stage_groups": batch.stage_groups, "metric": args.metric,
+           "metric_ms": [round(gr.metric_seconds * 1e3, 3) for gr in grids]}
     batch.close()
     for gr in reversed(grids):
         gr.close()

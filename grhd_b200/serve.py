@@ -105,11 +105,15 @@ class GpuEngine:
     host work per request) runs on a pool of host threads from the moment the request
     arrives, so admission only waits for it when it has not finished yet."""
 
-    def __init__(self, precision: str = "fp64", device: int = 0, host_workers: int = 8):
+    def __init__(self, precision: str = "fp64", device: int = 0, host_workers: int = 8, metric: str = "host"):
+        """metric: "host" builds each request's metric cache with its host set-up and
+        uploads it; "device" leaves it out of the host set-up and builds the tables on the
+        GPU (grhd2_gpu_set_metric_analytic)."""
         import torch
         torch.cuda.set_device(device)
         self.torch = torch
         self.precision = precision
+        self.metric = metric
         self.stream = torch.cuda.Stream(device=device)
         self._problems = {}  # request id -> Future of its Problem
         self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=host_workers)
@@ -131,7 +135,8 @@ class GpuEngine:
         GIL while the host library builds it)."""
         from .problem import Problem
         if req.id not in self._problems:
-            self._problems[req.id] = self._pool.submit(Problem.from_keys, req.problem, **req.keys)
+            self._problems[req.id] = self._pool.submit(Problem.from_keys, req.problem,
+                                                       metric_cache=self.metric == "host", **req.keys)
 
     def problem(self, req: Request):
         """The request's host-side set-up (metric tables, initial data), built once."""
@@ -153,7 +158,7 @@ class GpuEngine:
         pb = self.problem(req)
         del self._problems[req.id]
         ts = time.perf_counter()
-        g = GpuGrid(pb, precision=self.precision, upload_initial=False)
+        g = GpuGrid(pb, precision=self.precision, upload_initial=False, metric=self.metric)
         tu = time.perf_counter()
         g.upload(p=pb.prims_view())
         g.prim_to_cons()
@@ -331,16 +336,19 @@ def main(argv=None):
     ap.add_argument("--max-michel-cells", type=int, default=4096)
     ap.add_argument("--steps-per-round", type=int, default=16)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--metric", choices=["host", "device"], default="host",
+                    help="build each request's metric tables on the host (uploaded) or on the device")
     args = ap.parse_args(argv)
     reqs = make_stream(args.requests, args.seed, args.rate, args.michel_final_time,
                        riemann_cells=(128, args.max_riemann_cells), michel_cells=(512, args.max_michel_cells))
-    eng = GpuEngine(args.precision)
+    eng = GpuEngine(args.precision, metric=args.metric)
     srv = SolveServer(eng, steps_per_round=args.steps_per_round)
     res = srv.run(reqs)
     eng.close()
     out = summarize(res)
     out.update(peak_active=srv.peak_active, peak_bytes=srv.peak_bytes, rounds=srv.rounds, rebuilds=srv.rebuilds,
-               budget_bytes=srv.budget, precision=args.precision, host_s=srv.host_s, engine_host_s=eng.host_s)
+               budget_bytes=srv.budget, precision=args.precision, metric=args.metric, host_s=srv.host_s,
+               engine_host_s=eng.host_s)
     print(json.dumps(out))
 
 

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import time
 
 import numpy as np
 
@@ -34,14 +35,19 @@ class GpuGrid:
     """One grid on the GPU, built from a :class:`Problem` (or explicit config/tables)."""
 
     def __init__(self, problem: Problem, precision: str = "fp64", upload_initial: bool = True,
-                 stream: int | None = None):
+                 stream: int | None = None, metric: str = "host"):
         """stream: a cudaStream_t (integer) the handle launches on; None creates a private
-        one.  Grids that will step together in a :class:`GpuBatch` share one stream."""
+        one.  Grids that will step together in a :class:`GpuBatch` share one stream.
+        metric: "host" uploads the problem's metric cache (grhd2_gpu_set_metric); "device"
+        builds the same tables from the analytic metric on the GPU
+        (grhd2_gpu_set_metric_analytic)."""
+        if metric not in ("host", "device"):
+            raise ValueError(f"metric must be 'host' or 'device', not {metric!r}")
         self.lib = N.gpu_lib()
         self.problem = problem
         self.precision = precision
         self.cfg = problem.config(PRECISION[precision])
-        self._mv = problem.metric_view()
+        self._mv = problem.metric_view() if metric == "host" else None
         self._bv = problem.bc_view()
         h = C.c_void_p()
         if stream is None:
@@ -50,7 +56,13 @@ class GpuGrid:
             rc = self.lib.grhd2_gpu_create_on_stream(C.byref(self.cfg), C.c_void_p(stream), C.byref(h))
         self._h = h
         self._check(rc)
-        self._check(self.lib.grhd2_gpu_set_metric(self._h, C.byref(self._mv)))
+        t0 = time.perf_counter()
+        if metric == "host":
+            self._check(self.lib.grhd2_gpu_set_metric(self._h, C.byref(self._mv)))
+        else:
+            self._check(self.lib.grhd2_gpu_set_metric_analytic(self._h, C.byref(problem.metric_params())))
+        # wall time of the metric-table call (both return with the tables on the device)
+        self.metric_seconds = time.perf_counter() - t0
         self._check(self.lib.grhd2_gpu_set_bc_data(self._h, C.byref(self._bv)))
         if upload_initial:
             p0 = problem.initial_prims()
@@ -79,6 +91,17 @@ class GpuGrid:
 
     def __exit__(self, *a):
         self.close()
+
+    def metric_table(self, which: int) -> np.ndarray:
+        """The device metric table `which` (0 centre, 1-3 the x, y, z faces) as a
+        (fields, entries) array; empty for a direction without faces."""
+        n = C.c_size_t()
+        self._check(self.lib.grhd2_gpu_metric_table(self._h, which, None, 0, C.byref(n)))
+        out = np.empty(n.value, dtype=np.float64)
+        if n.value:
+            self._check(self.lib.grhd2_gpu_metric_table(self._h, which, N.dptr(out), out.size, None))
+        nfield = 74 if which == 0 else 21
+        return out.reshape(nfield, -1)
 
     # ---- the reference surface -------------------------------------------------------
     def upload(self, up: np.ndarray | None = None, p: np.ndarray | None = None):

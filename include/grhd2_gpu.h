@@ -21,6 +21,7 @@
 #ifndef GRHD2_GPU_H
 #define GRHD2_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -116,6 +117,33 @@ typedef struct grhd2_gpu grhd2_gpu;
 int grhd2_gpu_create(const grhd2_gpu_config *cfg, grhd2_gpu **out);
 /* Upload the metric cache tables (precalculate_metric_cache, initialization.f90:265). */
 int grhd2_gpu_set_metric(grhd2_gpu *h, const grhd2_gpu_metric_view *m);
+
+/* What the analytic metric-cache build needs beyond the handle's configuration (which
+ * supplies metric_kind, geom_kind, use_log_r, nx, ny, dx and dy). */
+typedef struct {
+  double bh_mass; /* M of the Eddington-Finkelstein and Kerr-Schild metrics (bh_mass key) */
+  double a_spin;  /* Kerr-Schild spin a (spin key)                                        */
+  double x_min;   /* first x face: r_min, or ln(r_min) on a logarithmic radial grid      */
+  double y_min;   /* first y face (theta_min on polar grids)                              */
+} grhd2_gpu_metric_params;
+/* Build the metric tables on the device instead of uploading them: the same quantities
+ * as precalculate_metric_cache (initialization.f90:265-391) from the analytic metrics
+ * (metrics.f90:94-1242) at the cell centres x_min + (i - 1/2) dx, y_min + (j - 1/2) dy and
+ * the faces x_min + i dx, y_min + j dy, k-invariant, one thread per (i, j) entry.  Drop-in
+ * for grhd2_gpu_set_metric where the caller has no host cache to hand over (the host then
+ * builds none).  The device's sin, cos and exp differ from the C library's by a few ulps, so
+ * the tables agree with a host-built cache to ~1e-15 relative (bit for bit for Minkowski
+ * Cartesian and cylindrical).  Asynchronous on the handle's stream except for a final
+ * check of the tables' symmetry; GRHD2_ERR_ARG for an unknown metric or geometry kind. */
+int grhd2_gpu_set_metric_analytic(grhd2_gpu *h, const grhd2_gpu_metric_params *mp);
+/* Copy a device metric table to the host: which = 0 the centre table (74 fields x nx*ny:
+ * lapse, shift, gamma_ij and gamma^ij upper triangles, sqrt(gamma), g^{mu nu},
+ * Gamma^0_{mu nu} and d_d g_{mu nu} upper triangles, d_mu ln(alpha), beta^i/alpha), which
+ * = 1, 2, 3 the x, y, z face table (21 fields x faces: lapse, normal shift, gamma_ij upper
+ * triangle, sqrt(gamma), gamma^dd, the face frame's 9 cofactors, frame flag, axis/pole
+ * flag).  n is the capacity of out in doubles; *n_out (may be NULL) receives the table's
+ * size, 0 for a direction without faces.  Synchronises the handle's stream. */
+int grhd2_gpu_metric_table(grhd2_gpu *h, int32_t which, double *out, size_t n, size_t *n_out);
 /* Upload per-case boundary data (cache_michel_injector, conditions.f90:229). */
 int grhd2_gpu_set_bc_data(grhd2_gpu *h, const grhd2_gpu_bc_view *b);
 /* Copy state in: up(5,nx,ny,nz) and/or p(5,-g:nx+g,-g:ny+g,-g:nz+g); either may be NULL.

@@ -35,6 +35,11 @@ typedef struct {
 /* Build a problem from .par text (problem = sod | michel | fishbone_equatorial | ...). On
  * failure returns a negative code and writes a message into err (if errlen > 0). */
 int grhd2_problem_create(const char *par_text, grhd2_problem **out, char *err, int errlen);
+/* grhd2_problem_create with flags.  GRHD2_PROBLEM_NO_METRIC_CACHE: build no host metric
+ * cache (the caller builds the tables on the device with grhd2_gpu_set_metric_analytic);
+ * grhd2_problem_metric then fills only x_face and y_face and returns GRHD2_ERR_STATE. */
+#define GRHD2_PROBLEM_NO_METRIC_CACHE 1u
+int grhd2_problem_create_ex(const char *par_text, uint32_t flags, grhd2_problem **out, char *err, int errlen);
 void grhd2_problem_destroy(grhd2_problem *pb);
 int grhd2_problem_config(const grhd2_problem *pb, int32_t precision_policy, grhd2_gpu_config *cfg);
 int grhd2_problem_metric(const grhd2_problem *pb, grhd2_gpu_metric_view *mv);
