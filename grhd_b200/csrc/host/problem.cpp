@@ -807,8 +807,8 @@ void set_initial_conditions(grhd2_problem &pb) {
   case 10: case 11: case 12: {
     double r_in = P.fm_rin * P.bh_mass, r_mx = P.fm_rmax * P.bh_mass;
     if (!fm_prepare(P, r_in, r_mx, pb.fm_l, pb.fm_w_in)) fail("invalid Fishbone-Moncrief model parameters");
-    // the centre metric from the cache, or evaluated here when the cache is built on the
-    // device (the same function at the same point: the same values)
+    // the centre metric from the cache (conditions.f90:450-452), or evaluated here when the
+    // cache is built on the device (the same function at the same point: the same values)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
         const double r = P.log_r ? std::exp(pb.X(i)) : pb.X(i);
