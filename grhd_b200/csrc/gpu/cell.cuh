@@ -126,10 +126,10 @@ __device__ __forceinline__ void c2p_count(unsigned long long *cnt, unsigned fl) 
 // Resident 128-thread blocks per SM the register allocation must allow.  The kernel waits
 // on dependent FP64 chains (con2prim) and scattered table loads, so more warps in flight
 // pay for a few spilled registers: measured on the 2.5D and 3D torus batches, 8 blocks
-// (64 registers) is fastest for FP64 and 6 (80 registers; 7 and 8 measured slower) for
-// the mixed policy.
+// (64 registers) is fastest for FP64 (6: -4 %, 4: -14 %) and 5 (96 registers, a third of
+// the spills of 6) for the mixed policy (6: -1 %, 4, 7 and 8 slower).
 template <class PT>
-constexpr int cell_min_blocks() { return sizeof(PT) == sizeof(double) ? 8 : 6; }
+constexpr int cell_min_blocks() { return sizeof(PT) == sizeof(double) ? 8 : 5; }
 
 // cp.async (sm_80+ asynchronous global->shared copy, cp-size 4, 8 or 16 bytes) and its
 // commit/wait; a thread waits for its own groups only.
