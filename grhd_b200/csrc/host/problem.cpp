@@ -1044,6 +1044,24 @@ int grhd2_host_metric_at(int32_t metric_kind, int32_t geom_kind, int32_t use_log
   return GRHD2_OK;
 }
 
+int grhd2_host_dust_state(int32_t use_log_r, double bh_mass, double dust_accretion_constant, double p_floor,
+                          double x, double *state) {
+  if (!state) return GRHD2_ERR_ARG;
+  Params P;
+  P.metric = EF;
+  P.geom = SPH;
+  P.log_r = use_log_r != 0;
+  P.bh_mass = bh_mass;
+  P.dust_c = dust_accretion_constant;
+  P.p_floor = p_floor;
+  try {
+    dust_state(P, x, state);
+  } catch (const ParError &) {
+    return GRHD2_ERR_ARG;
+  }
+  return GRHD2_OK;
+}
+
 int grhd2_host_fm_prepare(int32_t metric_kind, int32_t geom_kind, int32_t use_log_r, double bh_mass, double a_spin,
                           double r_in, double r_max, double *l_ang, double *w_in, int32_t *ok) {
   Params P;

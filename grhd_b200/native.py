@@ -169,6 +169,7 @@ HOST_SYMBOLS = {
     "grhd2_problem_eval_metric": (C.c_int, [_VP, C.c_double, C.c_double] + [c_double_p] * 8),
     "grhd2_host_metric_at": (C.c_int, [C.c_int32] * 3 + [C.c_double] * 2 + [C.c_int32] + [C.c_double] * 2
                              + [c_double_p] * 8),
+    "grhd2_host_dust_state": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, c_double_p]),
     "grhd2_host_fm_prepare": (C.c_int, [C.c_int32] * 3 + [C.c_double] * 4 + [c_double_p] * 2
                               + [C.POINTER(C.c_int32)]),
     "grhd2_host_fm_state": (C.c_int, [C.c_int32] * 3 + [C.c_double] * 11 + [c_double_p, C.POINTER(C.c_int32)]),

@@ -90,6 +90,12 @@ int grhd2_host_fm_state(int32_t metric_kind, int32_t geom_kind, int32_t use_log_
                         double a_spin, double adiabatic_index, double rho_floor, double p_floor,
                         double radius, double theta, double r_in, double K, double l_ang, double w_in,
                         double *state, int32_t *inside);
+/* evaluate_dust_accretion_state (conditions.f90:249-278) at the radial coordinate x (r, or
+ * log r on a logarithmic grid) with the module globals bh_mass, dust_accretion_constant and
+ * p_floor set directly, as tests/test_case_corrections.f90:186-232 sets them: state(5).
+ * GRHD2_ERR_ARG for the parameters the reference rejects (r <= 0, M <= 0, constant >= 0). */
+int grhd2_host_dust_state(int32_t use_log_r, double bh_mass, double dust_accretion_constant, double p_floor,
+                          double x, double *state);
 
 #ifdef __cplusplus
 }
