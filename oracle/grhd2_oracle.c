@@ -1528,7 +1528,7 @@ void orc_global_diagnostics(const orc_config *c, const orc_metric *m, const doub
 }
 
 /* metrics.f90:66-87 */
-static int horizon_radius(double mass, double spin, double *r_plus) {
+int orc_horizon_radius(double mass, double spin, double *r_plus) {
   if (mass < 0.0) return -1;
   double big = 1.0;
   if (mass * mass > big) big = mass * mass;
@@ -1540,13 +1540,57 @@ static int horizon_radius(double mass, double spin, double *r_plus) {
   return 0;
 }
 
-/* output.f90:743-768, 797-834, 837-850, 852-948 */
+/* output.f90:743-768 kerr_schild_spheroidal_position, with sin/cos of theta and phi given */
+static void ks_position(double r, double st, double ct, double sp, double cp, double spin, double *pos) {
+  if (fabs(st) <= 64.0 * DBL_EPSILON) {  /* both poles collapse exactly onto the axis */
+    pos[0] = 0.0; pos[1] = 0.0; pos[2] = copysign(fabs(r), ct);
+    return;
+  }
+  pos[0] = (r * cp - spin * sp) * st;
+  pos[1] = (r * sp + spin * cp) * st;
+  pos[2] = r * ct;
+}
+
+void orc_ks_spheroidal_position(double r, double theta, double phi, double spin, double *pos) {
+  ks_position(r, sin(theta), cos(theta), sin(phi), cos(phi), spin, pos);
+}
+
+/* output.f90:797-834 gw_cartesian_kinematics: coordinate rates alpha v - beta (the radial
+ * rate times r on a logarithmic grid), the Cartesian position and velocity of the
+ * Kerr-Schild spheroidal chart, and the flat-space Jacobian sigma sin(theta) */
+static void gw_kinematics(double r, double st, double ct, double sp, double cp, double spin, double alpha,
+                          const double *beta, const double *v, int use_log_r, double *pos, double *vel, double *jac) {
+  double rates[3];
+  for (int d = 0; d < 3; ++d) rates[d] = alpha * v[d] - beta[d];
+  if (use_log_r) rates[0] = r * rates[0];
+  ks_position(r, st, ct, sp, cp, spin, pos);
+  vel[0] = rates[0] * cp * st + rates[1] * (r * cp - spin * sp) * ct - rates[2] * (r * sp + spin * cp) * st;
+  vel[1] = rates[0] * sp * st + rates[1] * (r * sp + spin * cp) * ct + rates[2] * (r * cp - spin * sp) * st;
+  vel[2] = rates[0] * ct - r * rates[1] * st;
+  const double sigma = r * r + spin * spin * (ct * ct);
+  *jac = sigma * st;
+}
+
+void orc_gw_kinematics(double r, double theta, double phi, double spin, double alpha, const double *beta,
+                       const double *v, int use_log_r, double *pos, double *vel, double *jac) {
+  gw_kinematics(r, sin(theta), cos(theta), sin(phi), cos(phi), spin, alpha, beta, v, use_log_r, pos, vel, jac);
+}
+
+/* output.f90:837-850 finn_evans_cell_stress */
+void orc_finn_evans_stress(double rho, double pres, double mr3, const double *pos, const double *vel, double dV,
+                           double *ixx, double *iyy, double *ixy) {
+  *ixx = (2.0 * rho * (vel[0] * vel[0]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[0] * pos[0])) * dV;
+  *iyy = (2.0 * rho * (vel[1] * vel[1]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[1] * pos[1])) * dV;
+  *ixy = (2.0 * rho * vel[0] * vel[1] - 2.0 * rho * mr3 * pos[0] * pos[1]) * dV;
+}
+
+/* output.f90:852-948 */
 int orc_gw_strain(const orc_config *c, const orc_metric *m, const double *p, const double *xc, const double *yc,
                   const double *zc, int use_log_r, double bh_mass, double spin, double *out) {
   for (int q = 0; q < 5; ++q) out[q] = 0.0;
   if (c->metric_kind == ORC_METRIC_MINKOWSKI || bh_mass < 0.1) return 1;
   double r_h;
-  if (horizon_radius(bh_mass, spin, &r_h)) return -1;
+  if (orc_horizon_radius(bh_mass, spin, &r_h)) return -1;
   const lay_t L = mklay(c);
   double ixx = 0.0, iyy = 0.0, ixy = 0.0;
   for (int k = 1; k <= c->nz; ++k)
@@ -1560,30 +1604,17 @@ int orc_gw_strain(const orc_config *c, const orc_metric *m, const double *p, con
         pres = pres - c->p_floor; if (!(pres > 0.0)) pres = 0.0;
         if (rho <= 0.0 && pres <= 0.0) continue;
         const size_t q = cell(c, i, j);
-        const double alpha = m->alpha_c[q];
-        double rates[3];
-        for (int d = 0; d < 3; ++d) rates[d] = alpha * p[pidx(&L, 2 + d, i, j, k)] - m->beta_c[3 * q + d];
-        if (use_log_r) rates[0] = r * rates[0];
-        const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
-        double pos[3], vel[3];
-        if (fabs(st) <= 64.0 * DBL_EPSILON) {
-          pos[0] = 0.0; pos[1] = 0.0; pos[2] = copysign(fabs(r), ct);
-        } else {
-          pos[0] = (r * cp - spin * sp) * st;
-          pos[1] = (r * sp + spin * cp) * st;
-          pos[2] = r * ct;
-        }
-        vel[0] = rates[0] * cp * st + rates[1] * (r * cp - spin * sp) * ct - rates[2] * (r * sp + spin * cp) * st;
-        vel[1] = rates[0] * sp * st + rates[1] * (r * sp + spin * cp) * ct + rates[2] * (r * cp - spin * sp) * st;
-        vel[2] = rates[0] * ct - r * rates[1] * st;
-        const double sigma = r * r + spin * spin * (ct * ct);
-        const double jac = sigma * st;
+        const double v[3] = {p[pidx(&L, 2, i, j, k)], p[pidx(&L, 3, i, j, k)], p[pidx(&L, 4, i, j, k)]};
+        double pos[3], vel[3], jac, cx, cy, cxy;
+        gw_kinematics(r, sin(th), cos(th), sin(ph), cos(ph), spin, m->alpha_c[q], &m->beta_c[3 * q], v, use_log_r,
+                      pos, vel, &jac);
         const double dV = jac * (use_log_r ? r : 1.0) * c->dx * c->dy * c->dz;
         const double r2 = pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2];
         const double mr3 = bh_mass / (r2 * sqrt(r2));
-        ixx = ixx + (2.0 * rho * (vel[0] * vel[0]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[0] * pos[0])) * dV;
-        iyy = iyy + (2.0 * rho * (vel[1] * vel[1]) + 2.0 * pres - 2.0 * rho * mr3 * (pos[1] * pos[1])) * dV;
-        ixy = ixy + (2.0 * rho * vel[0] * vel[1] - 2.0 * rho * mr3 * pos[0] * pos[1]) * dV;
+        orc_finn_evans_stress(rho, pres, mr3, pos, vel, dV, &cx, &cy, &cxy);
+        ixx = ixx + cx;
+        iyy = iyy + cy;
+        ixy = ixy + cxy;
       }
   out[0] = (ixx - iyy) / 1000.0;
   out[1] = (2.0 * ixy) / 1000.0;

@@ -126,6 +126,18 @@ void orc_global_diagnostics(const orc_config *c, const orc_metric *m, const doub
  * the horizon radius is undefined (metrics.f90:66-87). */
 int orc_gw_strain(const orc_config *c, const orc_metric *m, const double *p, const double *xc, const double *yc,
                   const double *zc, int use_log_r, double bh_mass, double spin, double *out);
+/* The pieces of calc_gw_strain, exposed for the reference's GW tests
+ * (tests/test_gw_geometry.f90, tests/test_gw_stress.f90): event_horizon_radius
+ * (metrics.f90:66-87; -1 where it is undefined), kerr_schild_spheroidal_position
+ * (output.f90:743-768), gw_cartesian_kinematics (output.f90:797-834; v the Eulerian
+ * velocity, beta the shift, both in grid components) and finn_evans_cell_stress
+ * (output.f90:837-850). */
+int orc_horizon_radius(double mass, double spin, double *r_plus);
+void orc_ks_spheroidal_position(double r, double theta, double phi, double spin, double *pos);
+void orc_gw_kinematics(double r, double theta, double phi, double spin, double alpha, const double *beta,
+                       const double *v, int use_log_r, double *pos, double *vel, double *jac);
+void orc_finn_evans_stress(double rho, double pres, double mr3, const double *pos, const double *vel, double dV,
+                           double *ixx, double *iyy, double *ixy);
 /* number of OpenMP threads used by orc_run / orc_step (1 without OpenMP) */
 int orc_num_threads(void);
 /* the exp used by WENO3 (reconstruction.f90:169), exposed for its accuracy test */

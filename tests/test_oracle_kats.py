@@ -1,11 +1,14 @@
 """Pins the CPU oracle against the known-answer tests of the reference's own test programs.
 
 Each case restates one check of tests/test_hllc_fluxes.f90, tests/test_multidimensional_cfl.f90,
-tests/test_polar_boundaries.f90 or tests/test_case_corrections.f90 (file:line in the
-docstrings) with the same inputs and tolerances, run through the oracle.  The same KATs
-run through the GPU C-ABI in test_gpu_kats.py.
+tests/test_polar_boundaries.f90, tests/test_case_corrections.f90, tests/test_gw_geometry.f90
+or tests/test_gw_stress.f90 (file:line in the docstrings) with the same inputs and
+tolerances, run through the oracle.  The same flux, CFL and boundary KATs run through the
+GPU C-ABI in test_gpu_kats.py; the device's GW strain equals the oracle's
+(test_diagnostics.py).
 """
 import ctypes as C
+import math
 
 import numpy as np
 import pytest
@@ -304,3 +307,78 @@ def test_weno3_exp_accuracy():
         a, b = L.orc_exp(float(x)), float(np.exp(x))
         assert abs(a - b) <= np.spacing(b), (x, a, b)
     assert L.orc_exp(0.0) == 1.0
+
+
+# ---- tests/test_gw_geometry.f90, tests/test_gw_stress.f90 (calc_gw_strain's pieces) ----
+def _gw(r, th, ph, spin, alpha, beta, v, log_r):
+    pos, vel, jac = np.zeros(3), np.zeros(3), C.c_double()
+    B.lib().orc_gw_kinematics(r, th, ph, spin, alpha, _p(np.asarray(beta, dtype=float)),
+                              _p(np.asarray(v, dtype=float)), int(log_r), _p(pos), _p(vel), C.byref(jac))
+    return pos, vel, jac.value
+
+
+def _ks_position(r, th, ph, spin):
+    pos = np.zeros(3)
+    B.lib().orc_ks_spheroidal_position(r, th, ph, spin, _p(pos))
+    return pos
+
+
+def test_gw_horizon_radius():
+    """test_gw_geometry.f90:17-22: Schwarzschild, Kerr a = 0.9 and extremal horizons."""
+    L, r = B.lib(), C.c_double()
+    for spin, want in [(0.0, 2.0), (0.9, 1.0 + math.sqrt(0.19)), (1.0, 1.0)]:
+        assert L.orc_horizon_radius(1.0, spin, C.byref(r)) == 0
+        assert abs(r.value - want) <= 1e-14
+    assert L.orc_horizon_radius(1.0, 1.1, C.byref(r)) == -1  # beyond extremal: undefined
+
+
+def test_gw_cartesian_kinematics():
+    """test_gw_geometry.f90:24-104: a fluid at rest with the shift has no transport
+    velocity; the logarithmic grid's components give the same position and velocity; the
+    position equals the spheroidal VTK map; the flat Jacobian; the velocity is the chain
+    rule of the position (central differences, 2e-9); a = 0 is the spherical map; the
+    poles collapse exactly onto the axis."""
+    r, th, ph, spin, alpha = 7.0, 1.1, 0.7, 0.8, 0.8
+    beta = np.array([0.04, -0.02, 0.01])
+    _, vel, _ = _gw(r, th, ph, spin, alpha, beta, beta / alpha, False)
+    assert np.max(np.abs(vel)) <= 1e-14
+    v = np.array([0.03, -0.04, 0.05])
+    pos, vel, _ = _gw(r, th, ph, spin, alpha, beta, v, False)
+    bl, vl = beta.copy(), v.copy()
+    bl[0] /= r
+    vl[0] /= r
+    pos_l, vel_l, _ = _gw(r, th, ph, spin, alpha, bl, vl, True)
+    assert np.max(np.abs(pos_l - pos)) <= 1e-14
+    assert np.max(np.abs(vel_l - vel)) <= 1e-14
+
+    r, rates = 4.3, np.array([0.12, -0.03, 0.21])
+    zero = np.zeros(3)
+    pos, vel, jac = _gw(r, th, ph, spin, 1.0, zero, rates, False)
+    assert np.max(np.abs(_ks_position(r, th, ph, spin) - pos)) <= 1e-14
+    assert abs(jac - (r ** 2 + spin ** 2 * math.cos(th) ** 2) * math.sin(th)) <= 1e-13
+    eps = 1e-6
+    pp = _gw(r + eps * rates[0], th + eps * rates[1], ph + eps * rates[2], spin, 1.0, zero, zero, False)[0]
+    pm = _gw(r - eps * rates[0], th - eps * rates[1], ph - eps * rates[2], spin, 1.0, zero, zero, False)[0]
+    assert np.max(np.abs(vel - (pp - pm) / (2.0 * eps))) <= 2e-9
+    pos, _, jac = _gw(r, th, ph, 0.0, 1.0, zero, zero, False)
+    sph = [r * math.sin(th) * math.cos(ph), r * math.sin(th) * math.sin(ph), r * math.cos(th)]
+    assert np.max(np.abs(pos - sph)) <= 1e-13
+    assert abs(jac - r ** 2 * math.sin(th)) <= 1e-13
+    assert np.array_equal(_ks_position(r, 0.0, ph, spin), [0.0, 0.0, r])
+    assert np.array_equal(_ks_position(r, math.acos(-1.0), ph, spin), [0.0, 0.0, -r])
+
+
+def test_finn_evans_circular_orbit():
+    """test_gw_stress.f90: a point mass on a circular Keplerian orbit has the analytic
+    second derivative of its trace-free quadrupole (1e-13)."""
+    M, m, R, phase = 1.0, 0.2, 5.0, 0.37
+    om = math.sqrt(M / R ** 3)
+    pos = np.array([R * math.cos(phase), R * math.sin(phase), 0.0])
+    vel = np.array([-R * om * math.sin(phase), R * om * math.cos(phase), 0.0])
+    ixx, iyy, ixy = C.c_double(), C.c_double(), C.c_double()
+    B.lib().orc_finn_evans_stress(m, 0.0, M / R ** 3, _p(pos), _p(vel), 1.0, C.byref(ixx), C.byref(iyy),
+                                  C.byref(ixy))
+    amp = 2.0 * m * R ** 2 * om ** 2
+    assert abs(ixx.value - (-amp * math.cos(2 * phase))) <= 1e-13
+    assert abs(iyy.value - (amp * math.cos(2 * phase))) <= 1e-13
+    assert abs(ixy.value - (-amp * math.sin(2 * phase))) <= 1e-13
