@@ -2,8 +2,8 @@
 
 The oracle restates the reference's arithmetic in its own operation order without FMA
 contraction; the FP64 kernels do the same, so the FP64 results agree to round-off.  The
-stated bar (north star) is a relative L1 of at most 1e-12 per conserved variable with
-identical con2prim failure/floor counts; most cases here are bit-identical.
+parity bar is a relative L1 of at most 1e-12 per conserved variable with identical
+con2prim failure/floor counts; most cases here are bit-identical.
 """
 import numpy as np
 import pytest
@@ -89,7 +89,7 @@ def test_rhs_parity(maker, kw):
     r_g = g.calc_rhs()
     # WENO3 calls exp(); CUDA's and the host libm's differ by up to 1 ulp, and the flux
     # difference -(F_i - F_{i-1})/dx amplifies that in the pointwise RHS.  The bar is the
-    # north star's norm (relative L1 per variable); the pointwise maximum gets a loose bound.
+    # parity norm (relative L1 per variable); the pointwise maximum gets a loose bound.
     l1 = rel_l1(r_g, r_o)
     assert np.all(l1 <= 1e-12), f"rhs relative L1 per variable {l1}"
     scale = np.abs(r_o).reshape(-1, 5).max(axis=0)
