@@ -463,6 +463,7 @@ __device__ __forceinline__ void cell_item(const GridDev &G, unsigned ia, unsigne
 //   double up[NEQ][CELL_BS], u[NEQ][CELL_BS]; PT p[NEQ][CELL_BS];
 //   R f[2 * dirs][NEQ][CELL_BS]   (lower, upper face of each active direction)
 constexpr int CELL_BS_STAGE = 128;
+static_assert(CELL_BS_STAGE % 32 == 0, "sliced cell tiles are whole warps along i");
 // Staging pays for the mixed policy (measured on the 2.5D and 3D torus batches: cell
 // update -7 %); the FP64 kernel is bound by its FP64 instruction stream and runs as fast
 // with direct loads and no shared memory limiting its resident blocks.
