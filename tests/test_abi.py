@@ -49,3 +49,14 @@ def test_create_rejects_bad_configs_without_touching_the_device():
     rc = lib.grhd2_gpu_create(C.byref(c), C.byref(h))
     assert rc == -6 and b"nz must be even" in lib.grhd2_gpu_last_error(h)
     lib.grhd2_gpu_destroy(h)
+
+
+def test_metric_entries_reject_missing_arguments_without_touching_the_device():
+    """The device metric build and the table read-back check their arguments first."""
+    lib = N.gpu_lib()
+    mp = N.MetricParams(bh_mass=1.0, a_spin=0.0, x_min=0.0, y_min=0.0)
+    assert lib.grhd2_gpu_set_metric_analytic(None, C.byref(mp)) == -1
+    assert lib.grhd2_gpu_set_metric_analytic(None, None) == -1
+    n = C.c_size_t(7)
+    assert lib.grhd2_gpu_metric_table(None, 0, None, 0, C.byref(n)) == -1
+    assert n.value == 7  # untouched on an argument error
