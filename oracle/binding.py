@@ -82,6 +82,8 @@ def lib(libm_exp: bool = False, stopwatch: bool = False):
             "orc_gw_strain": (C.c_int, [P, M, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double, _dp]),
             "orc_mdot": (C.c_int, [P, M, _dp, _dp, C.c_int, _dp]),
             "orc_horizon_radius": (C.c_int, [C.c_double, C.c_double, _dp]),
+            "orc_root_brent": (C.c_double, [P, _dp, _dp]),
+            "orc_sources": (None, [P, M, _dp, C.c_int, C.c_int, _dp]),
             "orc_ks_spheroidal_position": (None, [C.c_double] * 4 + [_dp]),
             "orc_gw_kinematics": (None, [C.c_double] * 5 + [_dp, _dp, C.c_int, _dp, _dp, _dp]),
             "orc_finn_evans_stress": (None, [C.c_double] * 3 + [_dp, _dp, C.c_double, _dp, _dp, _dp]),

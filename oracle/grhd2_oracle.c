@@ -810,6 +810,10 @@ static void calc_sources(const orc_config *c, const orc_metric *m, const double 
   src[EQ_PR] = src[EQ_PR] * alpha;
 }
 
+void orc_sources(const orc_config *c, const orc_metric *m, const double *prim, int i, int j, double *src) {
+  calc_sources(c, m, prim, i, j, src);
+}
+
 /* ---------------------------------------------------------------------------------- */
 /* evolution.f90:30-191 calc_rhs                                                        */
 /* ---------------------------------------------------------------------------------- */
@@ -1044,6 +1048,10 @@ static double root_brent(const orc_config *c, const double *cs, const double *gi
   }
   return -1.0;
 }
+/* root_brent on its own, for the restatement cross-check (the Newton-bisection hybrid
+ * rarely falls back to it) */
+double orc_root_brent(const orc_config *c, const double *cs, const double *ginv) { return root_brent(c, cs, ginv); }
+
 /* equations.f90:249-340 root_safe_newton; *brent set when the Brent fallback ran */
 static double root_safe_newton(const orc_config *c, const double *cs, const double *ginv, int *brent) {
   const double x_acc = 1.0e-10, x1 = 1.0;

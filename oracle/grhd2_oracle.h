@@ -138,6 +138,12 @@ void orc_gw_kinematics(double r, double theta, double phi, double spin, double a
                        const double *v, int use_log_r, double *pos, double *vel, double *jac);
 void orc_finn_evans_stress(double rho, double pres, double mr3, const double *pos, const double *vel, double dV,
                            double *ixx, double *iyy, double *ixy);
+/* calc_sources (equations.f90:509-552) with calculate_stress_energy_tensor
+ * (metrics.f90:1251-1310) for one cell (i,j 1-based) and primitive state prim(5) */
+void orc_sources(const orc_config *c, const orc_metric *m, const double *prim, int i, int j, double *src);
+/* root_brent (equations.f90:339-424) alone, for its restatement cross-check: cs(5) the
+ * conserved state, ginv the inverse 3-metric (Fortran order) */
+double orc_root_brent(const orc_config *c, const double *cs, const double *ginv);
 /* number of OpenMP threads used by orc_run / orc_step (1 without OpenMP) */
 int orc_num_threads(void);
 /* the exp used by WENO3 (reconstruction.f90:169), exposed for its accuracy test */
