@@ -11,6 +11,7 @@ once here and committed:
   fullsize_torus3d_256x128x128_20.npz     3D Kerr-Schild torus 256 x 128 x 128, MP5 + HLLC +
                                   shock sensor, 20 steps
   fullsize_torus3d_128x64x64_500.npz      the 3D torus at 128 x 64 x 64, 500 steps
+  fullsize_torus3d_256x128x128_500.npz    the 3D torus at its full size and final step count
 
 For the tori each file holds the SHA-256 of the final conserved state (the bytes of up in
 the reference layout, u(5, nx, ny, nz) with the variable fastest, little-endian float64),
@@ -45,6 +46,7 @@ CASES = {
     "torus2p5d_400x1x200_2000": (lambda: torus_2p5d(nx=400, nz=200), dict(nsteps=2000), False),
     "torus3d_256x128x128_20": (lambda: torus_3d(nx=256, ny=128, nz=128), dict(nsteps=20), False),
     "torus3d_128x64x64_500": (lambda: torus_3d(nx=128, ny=64, nz=64), dict(nsteps=500), False),
+    "torus3d_256x128x128_500": (lambda: torus_3d(nx=256, ny=128, nz=128), dict(nsteps=500), False),
 }
 
 
