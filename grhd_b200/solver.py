@@ -35,12 +35,15 @@ class GpuGrid:
     """One grid on the GPU, built from a :class:`Problem` (or explicit config/tables)."""
 
     def __init__(self, problem: Problem, precision: str = "fp64", upload_initial: bool = True,
-                 stream: int | None = None, metric: str = "host"):
+                 stream: int | None = None, metric: str | None = None):
         """stream: a cudaStream_t (integer) the handle launches on; None creates a private
         one.  Grids that will step together in a :class:`GpuBatch` share one stream.
         metric: "host" uploads the problem's metric cache (grhd2_gpu_set_metric); "device"
         builds the same tables from the analytic metric on the GPU
-        (grhd2_gpu_set_metric_analytic)."""
+        (grhd2_gpu_set_metric_analytic); None picks "host" when the problem has a host
+        cache and "device" when it was built without one."""
+        if metric is None:
+            metric = "host" if problem.metric_cache else "device"
         if metric not in ("host", "device"):
             raise ValueError(f"metric must be 'host' or 'device', not {metric!r}")
         self.lib = N.gpu_lib()
